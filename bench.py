@@ -1,0 +1,323 @@
+#!/usr/bin/env python
+"""Benchmark: synaptic events/s of the 1M-neuron IF_cond_exp network on B200.
+
+Workload (the large IF_cond_exp configuration): 1,000,000 IF_cond_exp neurons
+(800k excitatory / 200k inhibitory), 1000 random synapses per neuron (1e9
+synapses; targets uniform without self-loops; weights exc ~U(0,4) nS, inh
+~U(0,51) nS stored negative; delays U{1..64} steps), e_rev_E 0, e_rev_I -80 mV,
+tau_syn_E 5, tau_syn_I 10 ms, dt 0.1 ms, 100,000 Poisson inputs at 5 Hz with
+100 targets each, fp32 state.  Parameters the configuration leaves open are
+taken from the 4000-neuron IF_curr_exp configuration (tau_m 20 ms, cm 0.2 nF,
+v_rest -60, v_thresh -50, v_reset -60 mV, tau_refrac 5 ms); Poisson synapses
+~U(0,100) nS with delay 1 step; v(0) ~ U(-60,-50) mV.  Conductances in uS.
+
+A step = one simulation time step (propagate + update); the network is built
+on the device by the fixed fan-out generator.  Inputs are larger than L2
+(8 GB synapse table); the per-neuron state (16 MB) stays L2-resident across
+steps as it does in any run of this network.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun (N > 1) each rank runs an independent replica (the path does not
+shard: replicas only), value = all ranks' events / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "syn-events/s @1M IF_cond_exp"
+UNIT = "syn-events/s"
+DT_MS = 0.1
+BYTES_PER_EVENT = 8      # int32 target + fp32 weight, delay implied by the bucket
+BYTES_PER_NEURON = 48    # 16 B state read + 16 B write + 8 B input read + 8 B clear
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--neurons", type=int, default=1_000_000)
+    ap.add_argument("--fanout", type=int, default=1000)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--acc", default="float", choices=["float", "fixed"])
+    ap.add_argument("--e2e-steps", type=int, default=1000)
+    ap.add_argument("--profile-steps", type=int, default=200)
+    ap.add_argument("--cpu-neurons", type=int, default=50_000)
+    ap.add_argument("--cpu-steps", type=int, default=300)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def cond_config(n: int, fanout: int):
+    """Generator blocks, populations and initial state of the benchmark network."""
+    import szsnn_b200 as sz
+    from szsnn_b200.network import GenBlock
+
+    p = n // 10
+    D = 64
+    ne = int(0.8 * n)
+    blocks = [GenBlock(0, ne, 0, n, fanout, 0.0, 0.004, 1.0, 1, D, True, 1),
+              GenBlock(ne, n - ne, 0, n, fanout, 0.0, 0.051, -1.0, 1, D, True, 2),
+              GenBlock(n, p, 0, n, 100, 0.0, 0.1, 1.0, 1, 1, False, 3)]
+    pv = sz.fold_dt(sz.if_params(v_rest=-60, cm=0.2, tau_m=20, tau_refrac=5, tau_syn_E=5, tau_syn_I=10,
+                                 v_reset=-60, v_thresh=-50, e_rev_E=0.0, e_rev_I=-80.0), DT_MS)
+    pops = [sz.Pop(sz.IF_COND_EXP, 0, n, pv),
+            sz.Pop(sz.POISSON, n, n + p, np.array([5.0 * DT_MS * 1e-3], np.float32), seed=20240)]
+    return n, p, D, blocks, pops
+
+
+def init_state(n, p, seed):
+    rng = np.random.default_rng(seed)
+    v0 = np.concatenate([rng.uniform(-60, -50, n), np.zeros(p)]).astype(np.float32)
+    fired = np.concatenate([np.full(n, 1e4), np.zeros(p)]).astype(np.float32)
+    return [v0, None, None, fired]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                line = out.stdout.strip().splitlines()[0]
+                self.samples.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.1)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and
+                          s[3 + i].lower() in ("active", "1")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(args, n_steps_warm=100):
+    """Oracle port, all host threads, on a bounded sample of the same network."""
+    import oracle
+    import szsnn_b200 as sz  # noqa: F401
+
+    threads = os.cpu_count() or 1
+    n, p, D, blocks, pops = cond_config(args.cpu_neurons, args.fanout)
+    csr = oracle.generate(blocks, args.seed, n + p, D)
+    on = oracle.OracleNet(n, p, D, pops, csr, state=init_state(n, p, args.seed))
+    on.run(n_steps_warm, nthreads=threads)
+    t0 = time.perf_counter()
+    steps = max(args.cpu_steps - n_steps_warm, 50)
+    _, ev = on.run(steps, nthreads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} IF_cond_exp neurons x {args.fanout} synapses + {p} Poisson x 100, same weights, "
+                      f"delays and rates as the 1M network; {steps} steps after {n_steps_warm} warm-up steps; "
+                      f"{ev} events in {dt:.2f} s"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    cb = cpu_baseline(args)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.cpu_steps, "warmup": 100, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "IF_cond_exp 1M x 1000 syn, Poisson 100k x 100, dt 0.1 ms (bounded CPU sample)",
+                       "neurons": args.cpu_neurons},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import szsnn_b200 as sz
+    from szsnn_b200 import _lib as L
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = tdist
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def allreduce(x, op):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    ctx = sz.Context(local_rank)
+    n, p, D, blocks, pops = cond_config(args.neurons, args.fanout)
+    acc = L.ACC_FIXED if args.acc == "fixed" else L.ACC_FLOAT
+    net = sz.Network(ctx, n, p, D, pops, state=init_state(n, p, args.seed + rank), acc_mode=acc, graph_chunk=100)
+    t0 = time.perf_counter()
+    net.generate(blocks, seed=args.seed + 1000 * rank)
+    gen_s = time.perf_counter() - t0
+
+    # warm-up (graph instantiation, initial transient)
+    net.run_device(args.warmup)
+    ctx.sync()
+    s0 = net.stats()
+    barrier()
+    ctx.sync()
+    import ctypes as C
+    lib = L.lib()
+    # CUDA events on the net's stream, through torch if present, else via the library timing
+    with ClockSampler(local_rank) as clk:
+        t_wall = time.perf_counter()
+        net.run_device(args.steps)
+        ctx.sync()
+        t_wall = time.perf_counter() - t_wall
+        _, _, total_ms = (C.c_double(), C.c_double(), C.c_double())
+        pm, um, tm = C.c_double(), C.c_double(), C.c_double()
+        lib.szsnn_net_timing(net.h, C.byref(pm), C.byref(um), C.byref(tm))
+    barrier()
+    s1 = net.stats()
+    ms_timed = tm.value if tm.value > 0 else t_wall * 1e3
+    events = s1["events"] - s0["events"]
+    spikes = s1["spikes"] - s0["spikes"]
+    ms_max = allreduce(ms_timed, dist.ReduceOp.MAX if dist else None)
+    ev_tot = allreduce(float(events), dist.ReduceOp.SUM if dist else None)
+    value = ev_tot / (ms_max / 1e3)
+
+    # end to end through the public API: host input words in, host raster out, every step
+    e2e_steps = min(args.e2e_steps, args.steps)
+    forced = np.zeros((e2e_steps, net.words), np.uint32)
+    s2 = net.stats()
+    barrier()
+    t_e2e = time.perf_counter()
+    raster = net.run(e2e_steps, forced_words=forced, raster=True)
+    ctx.sync()
+    t_e2e = time.perf_counter() - t_e2e
+    s3 = net.stats()
+    e2e_events = s3["events"] - s2["events"]
+    e2e_max = allreduce(t_e2e, dist.ReduceOp.MAX if dist else None)
+    e2e_tot = allreduce(float(e2e_events), dist.ReduceOp.SUM if dist else None)
+    del raster, forced
+
+    # per-kernel device time (CUDA events around each launch, no graph)
+    s4 = net.stats()
+    prop_ms, upd_ms, prof_ms = net.profile(args.profile_steps)
+    s5 = net.stats()
+    pev = s5["events"] - s4["events"]
+    steps_p = args.profile_steps
+    prop_bytes = pev * BYTES_PER_EVENT / steps_p
+    upd_bytes = n * BYTES_PER_NEURON
+    hbm, peak_kind = peaks()
+    prop_gbs = prop_bytes / (prop_ms / steps_p * 1e-3) / 1e9
+    upd_gbs = upd_bytes / (upd_ms / steps_p * 1e-3) / 1e9
+    if prop_ms >= upd_ms:
+        dom = {"kernel": "k_propagate", "achieved": prop_gbs, "bytes_per_launch": prop_bytes,
+               "us_per_launch": prop_ms / steps_p * 1e3}
+    else:
+        dom = {"kernel": "k_update", "achieved": upd_gbs, "bytes_per_launch": upd_bytes,
+               "us_per_launch": upd_ms / steps_p * 1e3}
+    roofline = {"bound": "hbm", "achieved": round(dom["achieved"], 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(dom["achieved"] / hbm, 4), "traffic": None, "kernel": dom["kernel"],
+                "peak_source": peak_kind,
+                "us_per_launch": round(dom["us_per_launch"], 3),
+                "algorithmic_bytes_per_launch": int(dom["bytes_per_launch"]),
+                "propagate": {"us_per_launch": round(prop_ms / steps_p * 1e3, 3), "gbs": round(prop_gbs, 1),
+                              "events_per_launch": pev / steps_p},
+                "update": {"us_per_launch": round(upd_ms / steps_p * 1e3, 3), "gbs": round(upd_gbs, 1)}}
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cb = cpu_baseline(args)
+        except Exception as e:  # the baseline is reported, not required
+            cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        steps = args.steps
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "IF_cond_exp 1M neurons x 1000 synapses (1e9), 100k Poisson x 100, "
+                                   "delays U{1..64} steps, dt 0.1 ms",
+                       "neurons": n, "sources": p, "synapses": net.n_synapses, "max_delay": D,
+                       "accumulation": args.acc, "graph_chunk": 100,
+                       "l2": "inputs larger than L2 (8 GB synapse table); neuron state L2-resident across steps",
+                       "parallelism": f"replicas x{world}"},
+            "neuron_updates_per_s": (n + p) * steps * world / (ms_max / 1e3),
+            "mean_rate_hz": spikes / max(n + p, 1) / (steps * DT_MS * 1e-3),
+            "events_per_step": events / steps,
+            "generate_s": gen_s,
+            "roofline": roofline,
+            "cpu_baseline": cb,
+            "e2e": {"value": e2e_tot / e2e_max, "unit": UNIT, "steps": e2e_steps,
+                    "h2d_bytes_per_step": int(net.words * 4), "d2h_bytes_per_step": int(net.words * 4),
+                    "api": "szsnn_net_run (host forced-spike words in, host raster out)"},
+            "gpu_launches": int(2 * steps + (steps + 99) // 100),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    net.close()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,318 @@
+/*
+ * szsnn_cuda.h -- C ABI of the B200 (sm_100a) implementation of SZSNN's
+ * clock-driven simulation step.
+ *
+ * The reference drives four OpenCL kernels through szsnn::Context
+ * (szsnn1.1/src/Context.hpp:77-303): createKernel / setKernelArg /
+ * enqueueKernel / createBuffer / writeBuffer / readBuffer and a single in-order
+ * command queue.  This header replaces that seam: plain pointers and sizes,
+ * one CUDA stream per context, every call returns a status code (0 = ok) and
+ * szsnn_last_error() gives the message (the reference throws SzsnnException on
+ * any CL status, szsnn1.1/src/utils.h:144-155).
+ *
+ * Ownership: device buffers returned by szsnn_alloc belong to the context
+ * until szsnn_free; host memory always belongs to the caller and is not
+ * retained after a call returns.  A context is not thread-safe: calls on one
+ * context must be serialised (the reference uses one host thread and one
+ * queue, szsnn1.1/src/Context.cpp:213).
+ *
+ * Three groups of entry points:
+ *  1. context and buffers                       (Context / DataBuffer seam)
+ *  2. drop-in kernels on the reference layout   (the four .cl kernels, same
+ *     argument lists, device pointers)
+ *  3. native network path (delay-bucketed CSR, device spike ring, Poisson
+ *     sources, IF_cond_exp, CUDA graphs), batched sweeps and the
+ *     IF_curr_exp adjoint used by the pyszsnn autograd function.
+ */
+#ifndef SZSNN_CUDA_H
+#define SZSNN_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define SZSNN_OK            0
+#define SZSNN_ERR_ARG       1   /* bad argument (null pointer, size, range)          */
+#define SZSNN_ERR_CUDA      2   /* CUDA runtime error                               */
+#define SZSNN_ERR_NOMEM     3   /* device or host allocation failed                 */
+#define SZSNN_ERR_LIMIT     4   /* layout limit of the reference format exceeded     */
+#define SZSNN_ERR_DEVICE    5   /* device-side check failed (overflow, bad index)    */
+#define SZSNN_ERR_TIMEOUT   6   /* bounded device wait expired                      */
+#define SZSNN_ERR_STATE     7   /* call not valid in the current state              */
+
+/* device-side sticky error codes (szsnn_device_error) */
+#define SZSNN_DEV_OK             0
+#define SZSNN_DEV_BAD_TARGET     1  /* synapse target outside the partition / network */
+#define SZSNN_DEV_QUEUE_OVERFLOW 2  /* global or local queue slot full                */
+#define SZSNN_DEV_RING_OVERFLOW  3  /* native spike ring slot full                    */
+#define SZSNN_DEV_NONFINITE      4  /* NaN/Inf found by szsnn_net_check_finite        */
+#define SZSNN_DEV_BAD_DELAY      5  /* delay outside 1..max_delay                     */
+
+typedef struct szsnn_ctx szsnn_ctx;
+typedef struct szsnn_net szsnn_net;
+typedef struct szsnn_layout szsnn_layout;
+
+/* Compile-time constants of the reference (szsnn1.1/src/locales.h:17-46),
+ * which it prepends to every kernel source (Context.cpp:260-274).  Here they
+ * are run-time values fixed at context creation. */
+typedef struct {
+    uint32_t max_partition_size;  /* MAX_PARTITION_SIZE (<= 1024, multiple of 32)   */
+    uint32_t threads_per_group;   /* THREADS_PER_GROUP = MPS / NEURONS_PER_WI        */
+    uint32_t warp_size;           /* WARP_SIZE == BUNDLE_SIZE (<= 32)                */
+    uint32_t max_synaptic_delay;  /* MAX_SYNAPTIC_DELAY (<= 64: uint64 delay bitmap) */
+} szsnn_layout_consts;
+
+/* --------------------------------------------- 1. context and buffers --- */
+/* Context::setup (Context.cpp:136-224): pick device, create the queue. */
+int szsnn_ctx_create(int device, const szsnn_layout_consts* consts, szsnn_ctx** out);
+int szsnn_ctx_destroy(szsnn_ctx* ctx);
+const char* szsnn_last_error(const szsnn_ctx* ctx);
+/* Use an external CUDA stream (cudaStream_t) instead of the context's own. */
+int szsnn_set_stream(szsnn_ctx* ctx, void* cuda_stream);
+void* szsnn_get_stream(szsnn_ctx* ctx);
+
+/* Context::createBuffer (Context.cpp:398-417) */
+int szsnn_alloc(szsnn_ctx* ctx, size_t bytes, void** dev_out);
+int szsnn_free(szsnn_ctx* ctx, void* dev);
+/* Context::writeBuffer / readBuffer with CL_TRUE (Context.cpp:421-505): blocking */
+int szsnn_h2d(szsnn_ctx* ctx, void* dev, const void* host, size_t bytes);
+int szsnn_d2h(szsnn_ctx* ctx, void* host, const void* dev, size_t bytes);
+int szsnn_memset(szsnn_ctx* ctx, void* dev, int value, size_t bytes);
+/* cl::Event::wait + CommandQueue::finish (Simulation.ipp:409-419); also
+ * reports the device-side sticky error as SZSNN_ERR_DEVICE. */
+int szsnn_sync(szsnn_ctx* ctx);
+int szsnn_device_error(szsnn_ctx* ctx, uint32_t* code_out, uint32_t* info_out);
+int szsnn_clear_device_error(szsnn_ctx* ctx);
+
+/* Options that replace the reference's -D kernel flags (Simulation.ipp:13-38). */
+#define SZSNN_OPT_OUTPUT_SPARSE_INPUT   1  /* input kernel stores sparse spikes
+                                              (-DSZSNN_KERNEL_OUTPUT_SPIKES, off when
+                                              SZSNN_NO_INPUT_TO_OUTPUT == 1, locales.h:64-68) */
+#define SZSNN_OPT_FIRED_OUTPUT_PARTS    2  /* partitions held by firedOutput: dense
+                                              spike words beyond it are not written
+                                              (the reference writes past the end for the
+                                              input partition, Const_rate_update_kernel.cl:238) */
+#define SZSNN_OPT_IZH_HALF_STEPS        3  /* Izhikevich: two 0.5 ms half-steps for v */
+int szsnn_set_option(szsnn_ctx* ctx, int option, int64_t value);
+
+/* ------------------------------ 2. drop-in kernels, reference layout ----
+ * Argument lists are those bound by Simulation::prep*Kernel
+ * (Simulation.ipp:214-340); all pointers are device pointers.  The launch
+ * covers the partitions the reference's NDRange covers: arg 1 partitions. */
+
+/* IF_curr_exp_update (cl/IF_curr_exp_update_kernel.cl:100-120) */
+int szsnn_update_if_curr_exp(szsnn_ctx* ctx, uint64_t cycle, uint32_t localPartitionCount,
+                             const uint32_t* partitionSizes, const float* neuronParams,
+                             float* neuronVars, uint32_t isInputCurrent, float* inputCurrent,
+                             float* current, uint32_t isInputFiring, uint32_t* inputFired,
+                             uint32_t* firedCount, uint32_t* fired, uint32_t* firedOutput,
+                             uint32_t partitionOffset, uint32_t globalPartitionCount);
+/* Izhikevich_update (cl/Izhikevich_update_kernel.cl:95-115) */
+int szsnn_update_izhikevich(szsnn_ctx* ctx, uint64_t cycle, uint32_t localPartitionCount,
+                            const uint32_t* partitionSizes, const float* neuronParams,
+                            float* neuronVars, uint32_t isInputCurrent, float* inputCurrent,
+                            float* current, uint32_t isInputFiring, uint32_t* inputFired,
+                            uint32_t* firedCount, uint32_t* fired, uint32_t* firedOutput,
+                            uint32_t partitionOffset, uint32_t globalPartitionCount);
+/* Const_rate_update (cl/Const_rate_update_kernel.cl:91-111) */
+int szsnn_update_const_rate(szsnn_ctx* ctx, uint64_t cycle, uint32_t localPartitionCount,
+                            const uint32_t* partitionSizes, const float* neuronParams,
+                            float* neuronVars, uint32_t isInputCurrent, float* inputCurrent,
+                            float* current, uint32_t isInputFiring, uint32_t* inputFired,
+                            uint32_t* firedCount, uint32_t* fired, uint32_t* firedOutput,
+                            uint32_t partitionOffset, uint32_t globalPartitionCount);
+/* gather (cl/gather_kernel.cl:67-77) */
+int szsnn_gather(szsnn_ctx* ctx, uint64_t cycle, uint32_t partitionCount,
+                 const uint32_t* partitionSizes, float* current, uint64_t gqPitch,
+                 uint32_t* gqBundleCounter, uint32_t* gqBundles, const uint32_t* targets,
+                 const float* weights);
+/* scatter (cl/scatter_kernel.cl:68-83); groupPtrs / groupMatrix are uint2
+ * arrays passed as uint32 pairs, lqEntries is a short2 array as int16 pairs. */
+int szsnn_scatter(szsnn_ctx* ctx, uint64_t cycle, uint32_t partitionCount,
+                  uint32_t* firedCount, uint32_t* fired, uint32_t groupPitch, uint32_t groupStep,
+                  const uint32_t* groupPtrs, const uint32_t* groupMatrix, uint64_t gqPitch,
+                  uint32_t* gqBundleCounter, uint32_t* gqBundles, uint32_t* lqEntryCounter,
+                  int16_t* lqEntries, const uint64_t* delayBits);
+
+/* Reference-layout builder (host only, no GPU needed): restates
+ * NeuronData/SynapseData/SynapseIndex/GroupData/GlobalQueue/LocalQueue/
+ * SpikeBuffer/CurrentData::initialize (NeuronData.ipp:27-170,
+ * SynapseData.ipp:8-111, SynapseIndex.cpp:42-63, GroupData.cpp:70-228,
+ * GlobalQueue.cpp:13-45, LocalQueue.cpp:32-70, SpikeBuffer.cpp:34-95,
+ * CurrentData.ipp:15-50).  Synapse ids are global ids: neurons 0..N-1 and
+ * inputs at Pn*MPS + i (NetworkGraph::connectInput, NetworkGraph.ipp:520-536).
+ * delay1 is the stored delay (user delay + 1, NetworkGraph.ipp:431). */
+typedef struct {
+    uint32_t n_neurons;
+    uint32_t n_inputs;
+    uint32_t neuron_param_count, neuron_var_count;  /* model traits (neuron_model_traits.hpp) */
+    uint32_t input_param_count, input_var_count;
+    const float* neuron_params;   /* [n_neurons][param_count] row-major, or NULL */
+    const float* neuron_vars;     /* [n_neurons][var_count]   */
+    const float* input_params;    /* [n_inputs][input_param_count] */
+    const float* input_vars;
+    uint64_t n_synapses;
+    const uint32_t* src;          /* global ids */
+    const uint32_t* tgt;
+    const float* weight;
+    const uint32_t* delay1;
+    uint32_t add_phony_synapse;   /* NetworkGraph::_addPhonySynapse (NetworkGraph.hpp:127-135) */
+} szsnn_layout_desc;
+
+/* array ids for szsnn_layout_array */
+enum {
+    SZSNN_L_PARTITION_SIZES = 0, /* uint32 [Ptot]                              */
+    SZSNN_L_NEURON_PARAMS,       /* float  [pc][Pn][MPS]                       */
+    SZSNN_L_NEURON_VARS,         /* float  [vc][Pn][MPS]                       */
+    SZSNN_L_INPUT_PARAMS,        /* float  [ipc][1][MPS]                       */
+    SZSNN_L_INPUT_VARS,          /* float  [ivc][1][MPS]                       */
+    SZSNN_L_TARGETS,             /* uint32 [bundles][BUNDLE]                   */
+    SZSNN_L_WEIGHTS,             /* float  [bundles][BUNDLE]                   */
+    SZSNN_L_DELAY_BITS,          /* uint64 [network size]                      */
+    SZSNN_L_GROUP_PTRS,          /* uint2  [Ptot][MPS][D]                      */
+    SZSNN_L_GROUP_MATRIX,        /* uint2  [words allocated]                   */
+    SZSNN_L_GQ_COUNTER,          /* uint32 [ALIGN(2*Ptot,32)]                  */
+    SZSNN_L_GQ_BUNDLES,          /* uint32 [2*Ptot][gq pitch]                  */
+    SZSNN_L_LQ_COUNTER,          /* uint32 [Ptot][D]                           */
+    SZSNN_L_LQ_ENTRIES,          /* short2 [Ptot][D][ALIGN(MPS*D,32)]          */
+    SZSNN_L_FIRED,               /* uint32 [Ptot][MPS]                         */
+    SZSNN_L_FIRED_COUNT,         /* uint32 [Ptot]                              */
+    SZSNN_L_FIRED_INPUT,         /* uint32 [Ptot][MPS/32]                      */
+    SZSNN_L_FIRED_OUTPUT,        /* uint32 [Ptot][MPS/32]                      */
+    SZSNN_L_INPUT_CURRENT,       /* float  [Ptot][MPS]                         */
+    SZSNN_L_CURRENT,             /* float  [2][Ptot][MPS]                      */
+    SZSNN_L_COUNT
+};
+typedef struct {
+    uint32_t neuron_partitions, input_partitions, total_partitions;
+    uint32_t group_pitch, group_step;
+    uint64_t gq_pitch;            /* max incoming bundles of a partition */
+    uint64_t bundles;             /* bundle rows incl. the unused row 0 */
+    uint64_t bytes[SZSNN_L_COUNT];
+} szsnn_layout_info;
+
+int szsnn_layout_build(const szsnn_layout_consts* consts, const szsnn_layout_desc* desc,
+                       szsnn_layout** out, char* err, size_t err_len);
+int szsnn_layout_info_get(const szsnn_layout* L, szsnn_layout_info* info);
+int szsnn_layout_array(const szsnn_layout* L, int which, void* dst, size_t dst_bytes);
+int szsnn_layout_free(szsnn_layout* L);
+
+/* ---------------------------------------------- 3. native network path --
+ * Units: neurons 0..N-1, then sources N..N+P-1.  Synapses are rows per unit,
+ * bucketed by delay m = 1..D (m = the reference's stored delay, user delay + 1):
+ * bucket (s, m) = [row_ptr[s*D + m-1], row_ptr[s*D + m]).  A spike emitted at
+ * step t over a delay-m synapse is integrated by the update of step t + m,
+ * as in the reference (scatter_kernel.cl:154,207; gather_kernel.cl:55-58). */
+enum {
+    SZSNN_IF_CURR_EXP = 0,
+    SZSNN_IF_COND_EXP = 1,
+    SZSNN_IZHIKEVICH  = 2,
+    SZSNN_POISSON     = 3,
+    SZSNN_CONST_RATE  = 4
+};
+#define SZSNN_MAX_POPS 16
+#define SZSNN_POP_IZH_HALF_STEPS 1u
+
+/* Parameter slots: IF_curr_exp 0 v_rest 1 cm 2 tau_m 3 tau_refrac 4 tau_syn_E
+ * 5 tau_syn_I 6 i_offset 7 v_reset 8 v_thresh (IF_curr_exp_NeuronModel.hpp:12-23);
+ * IF_cond_exp adds 9 e_rev_E 10 e_rev_I; Izhikevich 0 a 1 b 2 c 3 d;
+ * Poisson 0 p (spike probability per step); Const_rate 0 rate (steps).
+ * Times are in steps (dt folded, as the reference's kernels assume dt = 1).
+ * State slots: IF*: 0 v 1 Ie|ge 2 Ii|gi 3 steps-since-spike; Izhikevich 0 v 1 u;
+ * Const_rate 0 last. */
+typedef struct {
+    int32_t  model;
+    uint32_t flags;
+    int64_t  begin, end;
+    float    p[12];
+    const float* pn_host;   /* per-unit parameters SoA [slot][end-begin] (host), or NULL */
+    uint64_t seed;          /* Poisson stream key */
+} szsnn_pop_desc;
+
+#define SZSNN_ACC_FLOAT 0u  /* fp32 atomic accumulation (order not fixed)          */
+#define SZSNN_ACC_FIXED 1u  /* int64 fixed point, w*2^32 rounded: bit-reproducible */
+
+typedef struct {
+    int64_t  n_neurons, n_sources;
+    int32_t  max_delay;             /* D, 1..1024 */
+    int32_t  n_pops;
+    szsnn_pop_desc pops[SZSNN_MAX_POPS];
+    uint64_t n_synapses;
+    const uint64_t* row_ptr_host;   /* (N+P)*D+1, or NULL with szsnn_net_generate */
+    const int32_t*  tgt_host;
+    const float*    w_host;
+    const float*    state_host[4];  /* initial state slots (length N+P) or NULL = 0 */
+    uint32_t acc_mode;
+    uint32_t graph_chunk;           /* steps per captured CUDA graph (0 = 100) */
+    int64_t  raster_capacity;       /* device raster ring, steps (0 = graph_chunk) */
+} szsnn_net_desc;
+
+/* Fixed fan-out generator block (device-side; identical algorithm in the
+ * test oracle): rows src_begin.. get `fanout` synapses with target
+ * ~U{tgt range} (self excluded on request), w = w_sign*(w_lo + (w_hi-w_lo)*u),
+ * delay ~U{d_lo..d_hi}, stored stably bucketed by delay. */
+typedef struct {
+    int64_t  src_begin, src_count;
+    int64_t  tgt_begin, tgt_count;
+    int32_t  fanout;
+    int32_t  exclude_self;
+    float    w_lo, w_hi, w_sign;
+    int32_t  d_lo, d_hi;
+    uint32_t stream;
+    uint64_t syn_offset;
+} szsnn_gen_block;
+
+typedef struct {
+    int64_t  steps_done;
+    uint64_t events;          /* delivered synaptic events (non-zero weights) */
+    uint64_t spikes;          /* spikes of neurons and sources */
+    uint64_t graph_launches;
+    uint64_t kernel_launches;
+} szsnn_net_stats;
+
+int szsnn_net_create(szsnn_ctx* ctx, const szsnn_net_desc* desc, szsnn_net** out);
+int szsnn_net_generate(szsnn_net* net, const szsnn_gen_block* blocks, int n_blocks, uint64_t seed);
+int szsnn_net_destroy(szsnn_net* net);
+/* Simulation::stepAndFired(fInput) (Simulation.ipp:517-530): one step with
+ * optional host forced-spike words and external current, fired words out. */
+int szsnn_net_step(szsnn_net* net, const uint32_t* forced_host, const float* current_host,
+                   uint32_t* fired_host);
+/* `steps` steps in CUDA-graph chunks.  forced_host: [steps][words] or NULL;
+ * raster_host: [steps][words] output spike words or NULL. */
+int szsnn_net_run(szsnn_net* net, int64_t steps, const uint32_t* forced_host,
+                  uint32_t* raster_host);
+/* Same with device buffers: forced_dev [steps][words], current_dev [steps][N],
+ * raster_dev [steps][words]; any may be NULL.  Asynchronous on the stream. */
+int szsnn_net_run_device(szsnn_net* net, int64_t steps, const uint32_t* forced_dev,
+                         const float* current_dev, uint32_t* raster_dev);
+int szsnn_net_stats_get(szsnn_net* net, szsnn_net_stats* out);
+/* state slot k (length N+P) copy out / in (checkpoint) */
+int szsnn_net_get_state(szsnn_net* net, int slot, float* host);
+int szsnn_net_set_state(szsnn_net* net, int slot, const float* host);
+/* whole-simulation checkpoint: state, spike ring and clock into one blob */
+int szsnn_net_checkpoint_size(szsnn_net* net, uint64_t* bytes);
+int szsnn_net_checkpoint(szsnn_net* net, void* host_blob, uint64_t bytes);
+int szsnn_net_restore(szsnn_net* net, const void* host_blob, uint64_t bytes);
+/* copy the device CSR back (row_ptr (N+P)*D+1, tgt, w) -- checks the generator */
+int szsnn_net_get_synapses(szsnn_net* net, uint64_t* row_ptr, int32_t* tgt, float* w);
+/* scan the state slots for NaN/Inf: sets SZSNN_DEV_NONFINITE */
+int szsnn_net_check_finite(szsnn_net* net, int* finite_out);
+/* inputs integrated at the last step (debug/parity): in_exc, in_inh (N) */
+int szsnn_net_last_inputs(szsnn_net* net, float* in_exc, float* in_inh);
+
+/* per-kernel device time of `steps` directly launched steps (CUDA events around
+ * each kernel on the launching stream), summed over the steps, in ms */
+int szsnn_net_profile(szsnn_net* net, int64_t steps, double* propagate_ms, double* update_ms, double* total_ms);
+/* total_ms: device time (CUDA events on the stream) of the last szsnn_net_run /
+ * szsnn_net_run_device; propagate/update: the last szsnn_net_profile */
+int szsnn_net_timing(szsnn_net* net, double* propagate_ms, double* update_ms, double* total_ms);
+int szsnn_net_set_tuning(szsnn_net* net, int propagate_group, int propagate_blocks, int update_block);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,37 @@
+"""Build the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+  oracle/_build/liboracle.so   plain-C restatement (always)
+  oracle/_ref/libclemu_*.so    the reference's own .cl kernels under the CPU
+                               work-group emulator (only where the reference
+                               sources are present; see clemu/build_clemu.py)
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def build_oracle(force: bool = False) -> str:
+    out_dir = os.path.join(HERE, "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    lib = os.path.join(out_dir, "liboracle.so")
+    srcs = [os.path.join(HERE, f) for f in ("oracle.c", "oracle_step.inc", "oracle.h", "philox.h")]
+    if force or not os.path.exists(lib) or any(os.path.getmtime(s) > os.path.getmtime(lib) for s in srcs):
+        cmd = ["gcc", "-O2", "-std=gnu11", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-msse2",
+               "-shared", "-fPIC", "-o", lib, os.path.join(HERE, "oracle.c"), "-lm"]
+        subprocess.run(cmd, check=True)
+    return lib
+
+
+def build_all(force: bool = False) -> None:
+    build_oracle(force)
+    from .clemu.build_clemu import REF_ROOT, build_clemu
+    if os.path.isdir(REF_ROOT):
+        build_clemu(force)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv)

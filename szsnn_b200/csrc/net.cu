@@ -1,0 +1,1001 @@
+// net.cu -- native B200 network path.
+//
+// Design (replaces the reference's bundle/queue layout, which cannot hold a
+// 1e9-synapse network: GroupData.cpp:94 sizes groupPtrs for every
+// (neuron, delay) pair and pads every bundle to 32 slots):
+//  * synapses: one row per unit (neurons, then sources), each row bucketed by
+//    delay m = 1..D; interleaved {int32 target, fp32 weight} = 8 B per synapse
+//    (the delay is implied by the bucket);
+//  * spike ring: D+1 slots of compacted spike ids.  Step t's update appends to
+//    slot t % (D+1); step t's propagate delivers slot (t-m) % (D+1) over
+//    bucket m for m = 1..D.  This is the reference's per-delay ring
+//    (scatter_kernel.cl:154) with the fan-out done at delivery time, so the
+//    accumulation targets the current step's 2 x N input arrays only
+//    (L2-resident: 8 MB at N = 1e6);
+//  * propagate: grid-stride over (m, spike) work items, G lanes per bucket
+//    segment, fp32 `red` atomics into in_exc / in_inh split by weight sign
+//    (gather_kernel.cl:172-178), or int64 fixed-point atomics for
+//    bit-reproducible sums;
+//  * update: one thread per unit for neurons and sources (Poisson draws from
+//    Philox), consuming and clearing the inputs, spikes compacted with a warp
+//    ballot and one atomic per spiking warp, raster word written from the
+//    ballot;
+//  * steps captured in CUDA graphs of `chunk` steps; the step counter lives in
+//    device memory, so no host synchronisation happens between steps.
+#include "common.cuh"
+
+#include <cstring>
+#include <map>
+#include <tuple>
+
+struct PopDev {
+    int32_t model;
+    uint32_t flags;
+    int64_t begin, end;
+    float p[12];
+    const float* pn;
+    uint64_t seed;
+};
+
+struct NetDev {
+    int64_t N, U, words;
+    int32_t D, npops;
+    const PopDev* pops;
+    const unsigned long long* row_ptr;
+    const int2* syn;
+    float* st0;
+    float* st1;
+    float* st2;
+    float* st3;
+    float* in_e;
+    float* in_i;
+    long long* fx_e;
+    long long* fx_i;
+    uint32_t acc_mode;
+    uint32_t* ring_cnt;
+    int32_t* ring_ids;
+    const long long* clock;
+    unsigned long long* stats;  // [0] events, [1] spikes (all but the newest step)
+    uint32_t* err;
+    float* dbg_in_e;
+    float* dbg_in_i;
+};
+
+struct szsnn_net {
+    szsnn_ctx* ctx = nullptr;
+    int64_t N = 0, U = 0, words = 0;
+    int32_t D = 0, R = 0;
+    uint32_t acc_mode = 0;
+    int32_t npops = 0;
+    szsnn_pop_desc pops[SZSNN_MAX_POPS];
+    PopDev* d_pops = nullptr;
+    float* d_pn[SZSNN_MAX_POPS] = {};
+    uint64_t n_syn = 0;
+    unsigned long long* d_row_ptr = nullptr;
+    int2* d_syn = nullptr;
+    float* d_st[4] = {};
+    float* d_in_e = nullptr;
+    float* d_in_i = nullptr;
+    long long* d_fx_e = nullptr;
+    long long* d_fx_i = nullptr;
+    uint32_t* d_ring_cnt = nullptr;
+    int32_t* d_ring_ids = nullptr;
+    long long* d_clock = nullptr;
+    unsigned long long* d_stats = nullptr;
+    int chunk = 100;
+    uint32_t* d_forced_stage = nullptr;
+    float* d_current_stage = nullptr;
+    uint32_t* d_raster_stage = nullptr;
+    float* d_dbg_in = nullptr;
+    uint32_t* h_pinned_words = nullptr;  // pinned bounce buffer: chunk * words
+    std::map<std::tuple<int, int>, cudaGraphExec_t> graphs;
+    int64_t steps_done = 0;
+    uint64_t graph_launches = 0, kernel_launches = 0;
+    int prop_group = 16, prop_blocks = 0, upd_block = 256;
+    double t_prop_ms = 0, t_upd_ms = 0, t_total_ms = 0;
+    cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;  // around the last szsnn_net_run*
+    bool run_timed = false;
+};
+
+namespace {
+
+struct PopParams {
+    const PopDev* pd;
+    int64_t off, cnt;
+    __device__ __forceinline__ float operator()(int k) const
+    {
+        return pd->pn ? pd->pn[(int64_t)k * cnt + off] : pd->p[k];
+    }
+};
+
+__global__ void k_advance(long long* clock, int k) { *clock += k; }
+
+template <int G>
+__global__ void __launch_bounds__(256) k_propagate(NetDev nd, int k_off)
+{
+    __shared__ uint32_t s_pre[1025];
+    __shared__ unsigned long long s_ev;
+    const long long t = *nd.clock + k_off;
+    const int D = nd.D, R = D + 1;
+    for (int m = threadIdx.x + 1; m <= D; m += blockDim.x) {
+        long long tm = t - m;
+        s_pre[m] = (tm >= 0) ? nd.ring_cnt[tm % R] : 0u;
+    }
+    if (threadIdx.x == 0) { s_pre[0] = 0; s_ev = 0; }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // inclusive scan of counts over m = 1..D
+        uint32_t carry = 0;
+        const uint32_t lane = threadIdx.x;
+        for (int m0 = 1; m0 <= D; m0 += 32) {
+            int m = m0 + (int)lane;
+            uint32_t c = (m <= D) ? s_pre[m] : 0u;
+            uint32_t incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (uint32_t)o) incl += y;
+            }
+            if (m <= D) s_pre[m] = carry + incl;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+    }
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        nd.ring_cnt[t % R] = 0;                                  // slot filled by update(t)
+        if (t >= 1) atomicAdd(&nd.stats[1], (unsigned long long)(s_pre[1]));  // spikes of step t-1
+    }
+    const uint32_t total = s_pre[D];
+    const uint32_t lg = threadIdx.x % G;
+    const int64_t gid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int64_t ngroups = ((int64_t)gridDim.x * blockDim.x) / G;
+    uint32_t ev = 0;
+    for (int64_t item = gid; item < (int64_t)total; item += ngroups) {
+        int lo = 1, hi = D;  // first m with s_pre[m] > item
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if ((int64_t)s_pre[mid] > item) hi = mid; else lo = mid + 1;
+        }
+        const int m = lo;
+        const uint32_t j = (uint32_t)(item - s_pre[m - 1]);
+        const int64_t slot = (t - m) % R;
+        const int64_t s = nd.ring_ids[slot * nd.U + j];
+        const unsigned long long a = nd.row_ptr[s * D + (m - 1)];
+        const unsigned long long e = nd.row_ptr[s * D + m];
+        for (unsigned long long q = a + lg; q < e; q += G) {
+            const int2 sw = nd.syn[q];
+            const float w = __int_as_float(sw.y);
+            if (w != 0.0f) {
+                if ((unsigned long long)sw.x >= (unsigned long long)nd.N) {
+                    dev_error(nd.err, SZSNN_DEV_BAD_TARGET, (uint32_t)sw.x);
+                    continue;
+                }
+                ++ev;
+                if (nd.acc_mode == SZSNN_ACC_FIXED) {
+                    long long qv = __float2ll_rn(w * 4294967296.0f);
+                    atomicAdd((unsigned long long*)(w >= 0.0f ? &nd.fx_e[sw.x] : &nd.fx_i[sw.x]),
+                              (unsigned long long)qv);
+                } else {
+                    atomicAdd(w >= 0.0f ? &nd.in_e[sw.x] : &nd.in_i[sw.x], w);
+                }
+            }
+        }
+    }
+    // events: warp reduce, one shared atomic per warp, one global per block
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
+    if ((threadIdx.x & 31) == 0 && ev) atomicAdd(&s_ev, (unsigned long long)ev);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_ev) atomicAdd(&nd.stats[0], s_ev);
+}
+
+__global__ void __launch_bounds__(256) k_update(NetDev nd, int k_off, const uint32_t* forced, const float* current,
+                                                uint32_t* out_words)
+{
+    const long long t = *nd.clock + k_off;
+    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31;
+    bool spk = false;
+    if (id < nd.U) {
+        int pi = -1;
+        for (int i = 0; i < nd.npops; ++i) {
+            if (id >= nd.pops[i].begin && id < nd.pops[i].end) { pi = i; break; }
+        }
+        if (pi >= 0) {
+            const PopDev* pd = &nd.pops[pi];
+            PopParams p{pd, id - pd->begin, pd->end - pd->begin};
+            const bool f = forced ? ((forced[id >> 5] >> (id & 31)) & 1u) : false;
+            const int model = pd->model;
+            if (id < nd.N) {
+                float in_e, in_i;
+                if (nd.acc_mode == SZSNN_ACC_FIXED) {
+                    in_e = __ll2float_rn(nd.fx_e[id]) * (1.0f / 4294967296.0f);
+                    in_i = __ll2float_rn(nd.fx_i[id]) * (1.0f / 4294967296.0f);
+                    nd.fx_e[id] = 0;
+                    nd.fx_i[id] = 0;
+                } else {
+                    in_e = nd.in_e[id];
+                    in_i = nd.in_i[id];
+                    nd.in_e[id] = 0.0f;
+                    nd.in_i[id] = 0.0f;
+                }
+                if (nd.dbg_in_e) { nd.dbg_in_e[id] = in_e; nd.dbg_in_i[id] = in_i; }
+                const float i_ext = current ? current[id] : 0.0f;
+                if (model == SZSNN_IF_CURR_EXP || model == SZSNN_IF_COND_EXP) {
+                    float v = nd.st0[id], g1 = nd.st1[id], g2 = nd.st2[id], fr = nd.st3[id];
+                    if (model == SZSNN_IF_CURR_EXP) spk = sz_if_curr_exp(p, v, g1, g2, fr, in_e, in_i, i_ext, f);
+                    else spk = sz_if_cond_exp(p, v, g1, g2, fr, in_e, in_i, i_ext, f);
+                    nd.st0[id] = v; nd.st1[id] = g1; nd.st2[id] = g2; nd.st3[id] = fr;
+                } else if (model == SZSNN_IZHIKEVICH) {
+                    float v = nd.st0[id], u = nd.st1[id];
+                    spk = sz_izhikevich(p, v, u, in_e, in_i, i_ext, f, (pd->flags & SZSNN_POP_IZH_HALF_STEPS) != 0);
+                    nd.st0[id] = v; nd.st1[id] = u;
+                }
+            } else {
+                if (model == SZSNN_POISSON) {
+                    spk = sz_poisson_fires(pd->seed, id, t, p(0)) || f;
+                } else if (model == SZSNN_CONST_RATE) {
+                    float last = nd.st0[id];
+                    spk = sz_const_rate(p, last, f);
+                    nd.st0[id] = last;
+                }
+            }
+        }
+    }
+    const uint32_t ball = __ballot_sync(0xffffffffu, spk);
+    const int64_t wd = id >> 5;
+    if (lane == 0 && out_words && wd < nd.words) out_words[wd] = ball;
+    if (ball) {
+        const int R = nd.D + 1;
+        const int64_t slot = t % R;
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&nd.ring_cnt[slot], (uint32_t)__popc(ball));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (spk) {
+            uint32_t rank = __popc(ball & ((1u << lane) - 1u));
+            uint32_t pos = base + rank;
+            if (pos < (uint32_t)nd.U) nd.ring_ids[slot * nd.U + pos] = (int32_t)id;
+            else dev_error(nd.err, SZSNN_DEV_RING_OVERFLOW, (uint32_t)slot);
+        }
+    }
+}
+
+// ---- device generator (fixed fan-out), one warp per row
+struct GenDev {
+    int64_t src_begin, src_count, tgt_begin, tgt_count;
+    int32_t fanout, exclude_self;
+    float w_lo, w_hi, w_sign;
+    int32_t d_lo, d_hi;
+    uint32_t stream;
+    uint64_t syn_offset;
+    uint32_t k0, k1;
+};
+
+struct GenDraw { int64_t t; float w; int m; };
+
+__device__ __forceinline__ GenDraw gen_draw(const GenDev& g, int64_t s, int k)
+{
+    uint4 x = sz_philox((uint32_t)s, (uint32_t)k, g.stream, SZ_STREAM_GEN, g.k0, g.k1);
+    GenDraw d;
+    if (g.exclude_self && s >= g.tgt_begin && s < g.tgt_begin + g.tgt_count) {
+        d.t = g.tgt_begin + sz_bounded(x.x, (uint32_t)(g.tgt_count - 1));
+        if (d.t >= s) d.t += 1;
+    } else {
+        d.t = g.tgt_begin + sz_bounded(x.x, (uint32_t)g.tgt_count);
+    }
+    float span = g.w_hi - g.w_lo;
+    float mag = g.w_lo + span * sz_u24(x.y);
+    d.w = g.w_sign * mag;
+    d.m = g.d_lo + (int)sz_bounded(x.z, (uint32_t)(g.d_hi - g.d_lo + 1));
+    return d;
+}
+
+__global__ void __launch_bounds__(256) k_generate(GenDev g, int D, unsigned long long* row_ptr, int2* syn)
+{
+    extern __shared__ uint32_t s_hist[];
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t* h = s_hist + (threadIdx.x >> 5) * D;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int F = g.fanout;
+    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < g.src_count; r += nwarps) {
+        const int64_t s = g.src_begin + r;
+        const unsigned long long base = g.syn_offset + (unsigned long long)r * (unsigned long long)F;
+        for (int j = lane; j < D; j += 32) h[j] = 0;
+        __syncwarp();
+        for (int k = lane; k < F; k += 32) {
+            uint4 x = sz_philox((uint32_t)s, (uint32_t)k, g.stream, SZ_STREAM_GEN, g.k0, g.k1);
+            int m = g.d_lo + (int)sz_bounded(x.z, (uint32_t)(g.d_hi - g.d_lo + 1));
+            atomicAdd(&h[m - 1], 1u);
+        }
+        __syncwarp();
+        uint32_t carry = 0;
+        for (int j0 = 0; j0 < D; j0 += 32) {
+            int j = j0 + (int)lane;
+            uint32_t c = (j < D) ? h[j] : 0u;
+            uint32_t incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (uint32_t)o) incl += y;
+            }
+            if (j < D) {
+                h[j] = carry + incl - c;
+                row_ptr[s * D + j] = base + carry + incl - c;
+            }
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        __syncwarp();
+        for (int kb = 0; kb < F; kb += 32) {
+            const int k = kb + (int)lane;
+            const bool valid = k < F;
+            const uint32_t mask = __ballot_sync(0xffffffffu, valid);
+            GenDraw d{0, 0.0f, 1};
+            uint32_t peers = 0, rank = 0;
+            if (valid) {
+                d = gen_draw(g, s, k);
+                peers = __match_any_sync(mask, d.m);
+                rank = __popc(peers & ((1u << lane) - 1u));
+                syn[base + h[d.m - 1] + rank] = make_int2((int)d.t, __float_as_int(d.w));
+            }
+            __syncwarp();
+            if (valid && rank == 0) h[d.m - 1] += __popc(peers);
+            __syncwarp();
+        }
+    }
+}
+
+__global__ void k_fill_rows(unsigned long long* row_ptr, int64_t s0, int64_t s1, int D, unsigned long long v)
+{
+    for (int64_t i = s0 * D + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s1 * D;
+         i += (int64_t)gridDim.x * blockDim.x)
+        row_ptr[i] = v;
+}
+
+__global__ void k_check_finite(const float* a, int64_t n, uint32_t* flag)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (!isfinite(a[i])) { *flag = 1u; }
+}
+
+__global__ void k_pack_syn(const int32_t* tgt, const float* w, int2* syn, uint64_t n)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        syn[i] = make_int2(tgt[i], __float_as_int(w[i]));
+}
+
+__global__ void k_unpack_syn(const int2* syn, int32_t* tgt, float* w, uint64_t n)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        int2 v = syn[i];
+        tgt[i] = v.x;
+        w[i] = __int_as_float(v.y);
+    }
+}
+
+int num_sms(szsnn_ctx* ctx) { return ctx->num_sms > 0 ? ctx->num_sms : 148; }
+
+NetDev make_dev(szsnn_net* n)
+{
+    NetDev d{};
+    d.N = n->N; d.U = n->U; d.words = n->words; d.D = n->D; d.npops = n->npops;
+    d.pops = n->d_pops; d.row_ptr = n->d_row_ptr; d.syn = n->d_syn;
+    d.st0 = n->d_st[0]; d.st1 = n->d_st[1]; d.st2 = n->d_st[2]; d.st3 = n->d_st[3];
+    d.in_e = n->d_in_e; d.in_i = n->d_in_i; d.fx_e = n->d_fx_e; d.fx_i = n->d_fx_i;
+    d.acc_mode = n->acc_mode; d.ring_cnt = n->d_ring_cnt; d.ring_ids = n->d_ring_ids;
+    d.clock = n->d_clock; d.stats = n->d_stats; d.err = n->ctx->d_err;
+    d.dbg_in_e = nullptr; d.dbg_in_i = nullptr;
+    return d;
+}
+
+cudaError_t launch_propagate(szsnn_net* n, const NetDev& d, int k_off)
+{
+    int blocks = n->prop_blocks > 0 ? n->prop_blocks : num_sms(n->ctx) * 8;
+    cudaStream_t st = n->ctx->stream;
+    switch (n->prop_group) {
+    case 4: k_propagate<4><<<blocks, 256, 0, st>>>(d, k_off); break;
+    case 8: k_propagate<8><<<blocks, 256, 0, st>>>(d, k_off); break;
+    case 32: k_propagate<32><<<blocks, 256, 0, st>>>(d, k_off); break;
+    default: k_propagate<16><<<blocks, 256, 0, st>>>(d, k_off); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update(szsnn_net* n, const NetDev& d, int k_off, const uint32_t* forced, const float* cur,
+                          uint32_t* words)
+{
+    int bs = n->upd_block;
+    int64_t blocks = sz_div_up(n->U, bs);
+    k_update<<<(unsigned)blocks, bs, 0, n->ctx->stream>>>(d, k_off, forced, cur, words);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (!count) count = 1;
+    return cudaMalloc((void**)p, count * sizeof(T));
+}
+
+void free_net(szsnn_net* n)
+{
+    if (!n) return;
+    for (auto& kv : n->graphs) cudaGraphExecDestroy(kv.second);
+    n->graphs.clear();
+    cudaFree(n->d_pops);
+    for (int i = 0; i < SZSNN_MAX_POPS; ++i) cudaFree(n->d_pn[i]);
+    cudaFree(n->d_row_ptr);
+    cudaFree(n->d_syn);
+    for (int k = 0; k < 4; ++k) cudaFree(n->d_st[k]);
+    cudaFree(n->d_in_e);
+    cudaFree(n->d_in_i);
+    cudaFree(n->d_fx_e);
+    cudaFree(n->d_fx_i);
+    cudaFree(n->d_ring_cnt);
+    cudaFree(n->d_ring_ids);
+    cudaFree(n->d_clock);
+    cudaFree(n->d_stats);
+    cudaFree(n->d_forced_stage);
+    cudaFree(n->d_current_stage);
+    cudaFree(n->d_raster_stage);
+    cudaFree(n->d_dbg_in);
+    if (n->h_pinned_words) cudaFreeHost(n->h_pinned_words);
+    if (n->ev_run0) cudaEventDestroy(n->ev_run0);
+    if (n->ev_run1) cudaEventDestroy(n->ev_run1);
+    delete n;
+}
+
+}  // namespace
+
+#define NET_TRY(n, call)                                                                        \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return szsnn_set_error((n)->ctx, e_ == cudaErrorMemoryAllocation ? SZSNN_ERR_NOMEM   \
+                                                                            : SZSNN_ERR_CUDA,   \
+                                   std::string(#call) + ": " + cudaGetErrorString(e_));         \
+    } while (0)
+
+extern "C" int szsnn_net_create(szsnn_ctx* ctx, const szsnn_net_desc* d, szsnn_net** out)
+{
+    if (!ctx || !d || !out) return szsnn_set_error(ctx, SZSNN_ERR_ARG, "szsnn_net_create: null argument");
+    *out = nullptr;
+    if (d->n_neurons < 0 || d->n_sources < 0 || d->n_neurons + d->n_sources < 1)
+        return szsnn_set_error(ctx, SZSNN_ERR_ARG, "szsnn_net_create: no units");
+    if (d->n_neurons + d->n_sources > 0x7fffffffLL)
+        return szsnn_set_error(ctx, SZSNN_ERR_LIMIT, "szsnn_net_create: more than 2^31-1 units");
+    if (d->max_delay < 1 || d->max_delay > 1024)
+        return szsnn_set_error(ctx, SZSNN_ERR_ARG, "szsnn_net_create: max_delay outside 1..1024");
+    if (d->n_pops < 0 || d->n_pops > SZSNN_MAX_POPS)
+        return szsnn_set_error(ctx, SZSNN_ERR_ARG, "szsnn_net_create: n_pops outside 0..16");
+    if (d->acc_mode > 1) return szsnn_set_error(ctx, SZSNN_ERR_ARG, "szsnn_net_create: bad acc_mode");
+    const int64_t N = d->n_neurons, U = d->n_neurons + d->n_sources;
+    for (int i = 0; i < d->n_pops; ++i) {
+        const szsnn_pop_desc& p = d->pops[i];
+        if (p.begin < 0 || p.end > U || p.begin > p.end)
+            return szsnn_set_error(ctx, SZSNN_ERR_ARG, "pop " + std::to_string(i) + ": range outside the units");
+        bool neuron_model = p.model == SZSNN_IF_CURR_EXP || p.model == SZSNN_IF_COND_EXP || p.model == SZSNN_IZHIKEVICH;
+        bool source_model = p.model == SZSNN_POISSON || p.model == SZSNN_CONST_RATE;
+        if (!neuron_model && !source_model)
+            return szsnn_set_error(ctx, SZSNN_ERR_ARG, "pop " + std::to_string(i) + ": unknown model");
+        if (p.begin < p.end && neuron_model && p.end > N)
+            return szsnn_set_error(ctx, SZSNN_ERR_ARG, "pop " + std::to_string(i) + ": neuron model on source ids");
+        if (p.begin < p.end && source_model && p.begin < N)
+            return szsnn_set_error(ctx, SZSNN_ERR_ARG, "pop " + std::to_string(i) + ": source model on neuron ids");
+        for (int j = 0; j < i; ++j)
+            if (p.begin < d->pops[j].end && d->pops[j].begin < p.end)
+                return szsnn_set_error(ctx, SZSNN_ERR_ARG, "pops " + std::to_string(j) + " and " + std::to_string(i) + " overlap");
+    }
+    const int D = d->max_delay;
+    if (d->row_ptr_host) {  // host CSR: bucket pointers must be monotone and end at n_synapses
+        const uint64_t* rp = d->row_ptr_host;
+        const uint64_t cnt = (uint64_t)U * D;
+        if (rp[0] != 0 || rp[cnt] != d->n_synapses)
+            return szsnn_set_error(ctx, SZSNN_ERR_ARG, "row_ptr must start at 0 and end at n_synapses");
+        for (uint64_t i = 0; i < cnt; ++i)
+            if (rp[i + 1] < rp[i]) return szsnn_set_error(ctx, SZSNN_ERR_ARG, "row_ptr not monotone");
+        if (d->n_synapses && (!d->tgt_host || !d->w_host))
+            return szsnn_set_error(ctx, SZSNN_ERR_ARG, "tgt/w missing");
+    }
+
+    szsnn_net* n = new szsnn_net();
+    n->ctx = ctx;
+    n->N = N; n->U = U; n->words = sz_div_up(U, 32); n->D = D; n->R = D + 1;
+    n->acc_mode = d->acc_mode; n->npops = d->n_pops;
+    n->chunk = d->graph_chunk ? (int)d->graph_chunk : 100;
+    n->n_syn = d->n_synapses;
+    std::memcpy(n->pops, d->pops, sizeof(n->pops));
+    cudaStream_t st = ctx->stream;
+#define C(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { std::string m_ = std::string(#x) + ": " + cudaGetErrorString(e_); int code_ = e_ == cudaErrorMemoryAllocation ? SZSNN_ERR_NOMEM : SZSNN_ERR_CUDA; free_net(n); return szsnn_set_error(ctx, code_, m_); } } while (0)
+    // populations
+    PopDev hp[SZSNN_MAX_POPS];
+    std::memset(hp, 0, sizeof(hp));
+    for (int i = 0; i < d->n_pops; ++i) {
+        const szsnn_pop_desc& p = d->pops[i];
+        hp[i].model = p.model; hp[i].flags = p.flags; hp[i].begin = p.begin; hp[i].end = p.end;
+        std::memcpy(hp[i].p, p.p, sizeof(hp[i].p));
+        hp[i].seed = p.seed;
+        if (p.pn_host && p.end > p.begin) {
+            size_t cnt = (size_t)12 * (p.end - p.begin);
+            C(dalloc(&n->d_pn[i], cnt));
+            C(cudaMemcpyAsync(n->d_pn[i], p.pn_host, cnt * sizeof(float), cudaMemcpyHostToDevice, st));
+            hp[i].pn = n->d_pn[i];
+        }
+    }
+    C(dalloc(&n->d_pops, SZSNN_MAX_POPS));
+    C(cudaMemcpyAsync(n->d_pops, hp, sizeof(hp), cudaMemcpyHostToDevice, st));
+    // synapses
+    C(dalloc(&n->d_row_ptr, (size_t)U * D + 1));
+    C(dalloc(&n->d_syn, (size_t)n->n_syn));
+    if (d->row_ptr_host) {
+        C(cudaMemcpyAsync(n->d_row_ptr, d->row_ptr_host, ((size_t)U * D + 1) * 8, cudaMemcpyHostToDevice, st));
+        if (n->n_syn) {  // pack tgt/w into {int32, fp32} pairs in bounded chunks
+            const uint64_t CH = 1ull << 26;
+            int32_t* dt = nullptr;
+            float* dw = nullptr;
+            C(dalloc(&dt, (size_t)std::min<uint64_t>(CH, n->n_syn)));
+            C(dalloc(&dw, (size_t)std::min<uint64_t>(CH, n->n_syn)));
+            for (uint64_t o = 0; o < n->n_syn; o += CH) {
+                uint64_t c = std::min<uint64_t>(CH, n->n_syn - o);
+                C(cudaMemcpyAsync(dt, d->tgt_host + o, c * 4, cudaMemcpyHostToDevice, st));
+                C(cudaMemcpyAsync(dw, d->w_host + o, c * 4, cudaMemcpyHostToDevice, st));
+                k_pack_syn<<<1024, 256, 0, st>>>(dt, dw, n->d_syn + o, c);
+                C(cudaGetLastError());
+            }
+            C(cudaStreamSynchronize(st));
+            cudaFree(dt);
+            cudaFree(dw);
+        }
+    } else {
+        C(cudaMemsetAsync(n->d_row_ptr, 0, ((size_t)U * D + 1) * 8, st));
+    }
+    // state
+    for (int k = 0; k < 4; ++k) {
+        C(dalloc(&n->d_st[k], (size_t)U));
+        if (d->state_host[k]) C(cudaMemcpyAsync(n->d_st[k], d->state_host[k], (size_t)U * 4, cudaMemcpyHostToDevice, st));
+        else C(cudaMemsetAsync(n->d_st[k], 0, (size_t)U * 4, st));
+    }
+    C(dalloc(&n->d_in_e, (size_t)N)); C(cudaMemsetAsync(n->d_in_e, 0, (size_t)std::max<int64_t>(N, 1) * 4, st));
+    C(dalloc(&n->d_in_i, (size_t)N)); C(cudaMemsetAsync(n->d_in_i, 0, (size_t)std::max<int64_t>(N, 1) * 4, st));
+    if (n->acc_mode == SZSNN_ACC_FIXED) {
+        C(dalloc(&n->d_fx_e, (size_t)N)); C(cudaMemsetAsync(n->d_fx_e, 0, (size_t)std::max<int64_t>(N, 1) * 8, st));
+        C(dalloc(&n->d_fx_i, (size_t)N)); C(cudaMemsetAsync(n->d_fx_i, 0, (size_t)std::max<int64_t>(N, 1) * 8, st));
+    }
+    C(dalloc(&n->d_ring_cnt, (size_t)n->R)); C(cudaMemsetAsync(n->d_ring_cnt, 0, (size_t)n->R * 4, st));
+    C(dalloc(&n->d_ring_ids, (size_t)n->R * U));
+    C(dalloc(&n->d_clock, 1)); C(cudaMemsetAsync(n->d_clock, 0, 8, st));
+    C(dalloc(&n->d_stats, 4)); C(cudaMemsetAsync(n->d_stats, 0, 32, st));
+    C(dalloc(&n->d_forced_stage, (size_t)n->chunk * n->words));
+    C(dalloc(&n->d_current_stage, (size_t)n->chunk * std::max<int64_t>(N, 1)));
+    C(dalloc(&n->d_raster_stage, (size_t)n->chunk * n->words));
+    C(dalloc(&n->d_dbg_in, (size_t)2 * std::max<int64_t>(N, 1)));
+    C(cudaMallocHost((void**)&n->h_pinned_words, (size_t)n->chunk * n->words * 4));
+    C(cudaEventCreate(&n->ev_run0));
+    C(cudaEventCreate(&n->ev_run1));
+    C(cudaStreamSynchronize(st));
+#undef C
+    *out = n;
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_destroy(szsnn_net* n)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    cudaStreamSynchronize(n->ctx->stream);
+    free_net(n);
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_generate(szsnn_net* n, const szsnn_gen_block* blocks, int nb, uint64_t seed)
+{
+    if (!n || (nb > 0 && !blocks) || nb < 0) return szsnn_set_error(n ? n->ctx : nullptr, SZSNN_ERR_ARG, "szsnn_net_generate: bad arguments");
+    cudaStream_t st = n->ctx->stream;
+    const int D = n->D;
+    // blocks must be sorted by src_begin and disjoint; synapse offsets are cumulative
+    uint64_t off = 0;
+    int64_t row = 0;
+    for (int i = 0; i < nb; ++i) {
+        const szsnn_gen_block& b = blocks[i];
+        if (b.src_begin < row || b.src_count < 0 || b.src_begin + b.src_count > n->U || b.fanout < 0 ||
+            b.d_lo < 1 || b.d_hi > D || b.d_lo > b.d_hi || b.tgt_begin < 0 || b.tgt_count < 1 ||
+            b.tgt_begin + b.tgt_count > n->N || (b.exclude_self && b.tgt_count < 2))
+            return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "szsnn_net_generate: bad block " + std::to_string(i));
+        if (b.src_begin > row) {
+            k_fill_rows<<<256, 256, 0, st>>>(n->d_row_ptr, row, b.src_begin, D, off);
+            NET_TRY(n, cudaGetLastError());
+        }
+        off += (uint64_t)b.src_count * (uint64_t)b.fanout;
+        row = b.src_begin + b.src_count;
+    }
+    if (row < n->U) {
+        k_fill_rows<<<256, 256, 0, st>>>(n->d_row_ptr, row, n->U, D, off);
+        NET_TRY(n, cudaGetLastError());
+    }
+    if (off != n->n_syn) {  // (re)allocate synapse storage for the generated count
+        NET_TRY(n, cudaStreamSynchronize(st));
+        cudaFree(n->d_syn);
+        n->d_syn = nullptr;
+        NET_TRY(n, dalloc(&n->d_syn, (size_t)off));
+        n->n_syn = off;
+    }
+    const unsigned long long total = off;
+    NET_TRY(n, cudaMemcpyAsync(n->d_row_ptr + (size_t)n->U * D, &total, 8, cudaMemcpyHostToDevice, st));
+    off = 0;
+    const size_t smem = (size_t)8 * D * 4;
+    if (smem > 48 * 1024) NET_TRY(n, cudaFuncSetAttribute(k_generate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int i = 0; i < nb; ++i) {
+        const szsnn_gen_block& b = blocks[i];
+        GenDev g{b.src_begin, b.src_count, b.tgt_begin, b.tgt_count, b.fanout, b.exclude_self,
+                 b.w_lo, b.w_hi, b.w_sign, b.d_lo, b.d_hi, b.stream, off,
+                 (uint32_t)seed, (uint32_t)(seed >> 32)};
+        if (b.src_count > 0) {
+            int64_t blocks_needed = sz_div_up(b.src_count, 8);
+            int grid = (int)std::min<int64_t>(blocks_needed, (int64_t)num_sms(n->ctx) * 16);
+            k_generate<<<grid, 256, smem, st>>>(g, D, n->d_row_ptr, n->d_syn);
+            NET_TRY(n, cudaGetLastError());
+        }
+        off += (uint64_t)b.src_count * (uint64_t)b.fanout;
+    }
+    NET_TRY(n, cudaStreamSynchronize(st));
+    return SZSNN_OK;
+}
+
+static int net_stage_step_inputs(szsnn_net* n, const uint32_t* forced_host, const float* current_host)
+{
+    cudaStream_t st = n->ctx->stream;
+    if (forced_host)
+        NET_TRY(n, cudaMemcpyAsync(n->d_forced_stage, forced_host, (size_t)n->words * 4, cudaMemcpyHostToDevice, st));
+    if (current_host && n->N)
+        NET_TRY(n, cudaMemcpyAsync(n->d_current_stage, current_host, (size_t)n->N * 4, cudaMemcpyHostToDevice, st));
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_step(szsnn_net* n, const uint32_t* forced_host, const float* current_host,
+                              uint32_t* fired_host)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    int rc = net_stage_step_inputs(n, forced_host, current_host);
+    if (rc) return rc;
+    NetDev d = make_dev(n);
+    d.dbg_in_e = n->d_dbg_in;
+    d.dbg_in_i = n->d_dbg_in + std::max<int64_t>(n->N, 1);
+    cudaStream_t st = n->ctx->stream;
+    NET_TRY(n, launch_propagate(n, d, 0));
+    NET_TRY(n, launch_update(n, d, 0, forced_host ? n->d_forced_stage : nullptr,
+                             current_host ? n->d_current_stage : nullptr, n->d_raster_stage));
+    k_advance<<<1, 1, 0, st>>>(n->d_clock, 1);
+    NET_TRY(n, cudaGetLastError());
+    n->kernel_launches += 3;
+    n->steps_done += 1;
+    if (fired_host) {
+        NET_TRY(n, cudaMemcpyAsync(n->h_pinned_words, n->d_raster_stage, (size_t)n->words * 4, cudaMemcpyDeviceToHost, st));
+        NET_TRY(n, cudaStreamSynchronize(st));
+        std::memcpy(fired_host, n->h_pinned_words, (size_t)n->words * 4);
+    }
+    return SZSNN_OK;
+}
+
+// graph of `len` steps; flags bit0 forced, bit1 current, bit2 raster
+static int net_graph(szsnn_net* n, int len, int flags, cudaGraphExec_t* out)
+{
+    auto key = std::make_tuple(len, flags);
+    auto it = n->graphs.find(key);
+    if (it != n->graphs.end()) { *out = it->second; return SZSNN_OK; }
+    cudaStream_t st = n->ctx->stream;
+    NetDev d = make_dev(n);
+    cudaGraph_t g = nullptr;
+    NET_TRY(n, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < len && e == cudaSuccess; ++k) {
+        e = launch_propagate(n, d, k);
+        if (e != cudaSuccess) break;
+        e = launch_update(n, d, k, (flags & 1) ? n->d_forced_stage + (size_t)k * n->words : nullptr,
+                          (flags & 2) ? n->d_current_stage + (size_t)k * std::max<int64_t>(n->N, 1) : nullptr,
+                          (flags & 4) ? n->d_raster_stage + (size_t)k * n->words : nullptr);
+    }
+    if (e == cudaSuccess) {
+        k_advance<<<1, 1, 0, st>>>(n->d_clock, len);
+        e = cudaGetLastError();
+    }
+    cudaError_t e2 = cudaStreamEndCapture(st, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return szsnn_set_error(n->ctx, SZSNN_ERR_CUDA,
+                               std::string("graph capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    NET_TRY(n, e);
+    n->graphs[key] = ex;
+    *out = ex;
+    return SZSNN_OK;
+}
+
+static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, const float* current, uint32_t* raster,
+                        bool host)
+{
+    if (!n || steps < 0) return SZSNN_ERR_ARG;
+    cudaStream_t st = n->ctx->stream;
+    NET_TRY(n, cudaEventRecord(n->ev_run0, st));
+    const cudaMemcpyKind in_kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    for (int64_t done = 0; done < steps;) {
+        const int len = (int)std::min<int64_t>(n->chunk, steps - done);
+        const int flags = (forced ? 1 : 0) | (current ? 2 : 0) | (raster ? 4 : 0);
+        if (forced) {
+            const size_t bytes = (size_t)len * n->words * 4;
+            if (host) {  // through the pinned bounce buffer so the copy is a true async DMA
+                NET_TRY(n, cudaStreamSynchronize(st));
+                std::memcpy(n->h_pinned_words, forced + (size_t)done * n->words, bytes);
+                NET_TRY(n, cudaMemcpyAsync(n->d_forced_stage, n->h_pinned_words, bytes, cudaMemcpyHostToDevice, st));
+            } else {
+                NET_TRY(n, cudaMemcpyAsync(n->d_forced_stage, forced + (size_t)done * n->words, bytes, in_kind, st));
+            }
+        }
+        if (current && n->N)
+            NET_TRY(n, cudaMemcpyAsync(n->d_current_stage, current + (size_t)done * n->N, (size_t)len * n->N * 4, in_kind, st));
+        cudaGraphExec_t ex;
+        int rc = net_graph(n, len, flags, &ex);
+        if (rc) return rc;
+        NET_TRY(n, cudaGraphLaunch(ex, st));
+        n->graph_launches += 1;
+        n->kernel_launches += (uint64_t)2 * len + 1;
+        if (raster) {
+            const size_t bytes = (size_t)len * n->words * 4;
+            if (host) {
+                NET_TRY(n, cudaMemcpyAsync(n->h_pinned_words, n->d_raster_stage, bytes, cudaMemcpyDeviceToHost, st));
+                NET_TRY(n, cudaStreamSynchronize(st));
+                std::memcpy(raster + (size_t)done * n->words, n->h_pinned_words, bytes);
+            } else {
+                NET_TRY(n, cudaMemcpyAsync(raster + (size_t)done * n->words, n->d_raster_stage, bytes,
+                                           cudaMemcpyDeviceToDevice, st));
+            }
+        }
+        done += len;
+        n->steps_done += len;
+    }
+    NET_TRY(n, cudaEventRecord(n->ev_run1, st));
+    n->run_timed = true;
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_run(szsnn_net* n, int64_t steps, const uint32_t* forced_host, uint32_t* raster_host)
+{
+    return net_run_impl(n, steps, forced_host, nullptr, raster_host, true);
+}
+
+extern "C" int szsnn_net_run_device(szsnn_net* n, int64_t steps, const uint32_t* forced_dev, const float* current_dev,
+                                    uint32_t* raster_dev)
+{
+    return net_run_impl(n, steps, forced_dev, current_dev, raster_dev, false);
+}
+
+// Per-kernel device time: `steps` steps launched directly (no graph), with
+// CUDA events on the launching stream around every kernel.
+extern "C" int szsnn_net_profile(szsnn_net* n, int64_t steps, double* prop_ms, double* upd_ms, double* total_ms)
+{
+    if (!n || steps < 1) return SZSNN_ERR_ARG;
+    cudaStream_t st = n->ctx->stream;
+    NetDev d = make_dev(n);
+    std::vector<cudaEvent_t> ev((size_t)(2 * steps + 1));
+    for (auto& e : ev) NET_TRY(n, cudaEventCreate(&e));
+    NET_TRY(n, cudaEventRecord(ev[0], st));
+    for (int64_t k = 0; k < steps; ++k) {
+        NET_TRY(n, launch_propagate(n, d, 0));
+        NET_TRY(n, cudaEventRecord(ev[(size_t)(2 * k + 1)], st));
+        NET_TRY(n, launch_update(n, d, 0, nullptr, nullptr, nullptr));
+        k_advance<<<1, 1, 0, st>>>(n->d_clock, 1);
+        NET_TRY(n, cudaEventRecord(ev[(size_t)(2 * k + 2)], st));
+        n->steps_done += 1;
+        n->kernel_launches += 3;
+    }
+    NET_TRY(n, cudaEventSynchronize(ev.back()));
+    double p = 0, u = 0;
+    for (int64_t k = 0; k < steps; ++k) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ev[(size_t)(2 * k)], ev[(size_t)(2 * k + 1)]);
+        cudaEventElapsedTime(&b, ev[(size_t)(2 * k + 1)], ev[(size_t)(2 * k + 2)]);
+        p += a;
+        u += b;
+    }
+    float tot = 0;
+    cudaEventElapsedTime(&tot, ev[0], ev.back());
+    for (auto& e : ev) cudaEventDestroy(e);
+    n->t_prop_ms = p;
+    n->t_upd_ms = u;
+    if (prop_ms) *prop_ms = p;
+    if (upd_ms) *upd_ms = u;
+    if (total_ms) *total_ms = tot;
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_timing(szsnn_net* n, double* prop_ms, double* upd_ms, double* total_ms)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    if (n->run_timed) {  // device time of the last szsnn_net_run / szsnn_net_run_device
+        NET_TRY(n, cudaEventSynchronize(n->ev_run1));
+        float ms = 0;
+        NET_TRY(n, cudaEventElapsedTime(&ms, n->ev_run0, n->ev_run1));
+        n->t_total_ms = ms;
+    }
+    if (prop_ms) *prop_ms = n->t_prop_ms;
+    if (upd_ms) *upd_ms = n->t_upd_ms;
+    if (total_ms) *total_ms = n->t_total_ms;
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_set_tuning(szsnn_net* n, int group, int blocks, int upd_block)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    if (group != 0 && group != 4 && group != 8 && group != 16 && group != 32)
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "propagate group must be 4, 8, 16 or 32");
+    if (upd_block != 0 && (upd_block < 32 || upd_block > 1024 || upd_block % 32))
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "update block must be a multiple of 32 in 32..1024");
+    if (group) n->prop_group = group;
+    if (blocks >= 0) n->prop_blocks = blocks;
+    if (upd_block) n->upd_block = upd_block;
+    for (auto& kv : n->graphs) cudaGraphExecDestroy(kv.second);
+    n->graphs.clear();
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_stats_get(szsnn_net* n, szsnn_net_stats* out)
+{
+    if (!n || !out) return SZSNN_ERR_ARG;
+    cudaStream_t st = n->ctx->stream;
+    unsigned long long s[4] = {0, 0, 0, 0};
+    long long clock = 0;
+    uint32_t newest = 0;
+    NET_TRY(n, cudaMemcpyAsync(s, n->d_stats, sizeof(s), cudaMemcpyDeviceToHost, st));
+    NET_TRY(n, cudaMemcpyAsync(&clock, n->d_clock, 8, cudaMemcpyDeviceToHost, st));
+    NET_TRY(n, cudaStreamSynchronize(st));
+    if (clock >= 1) {
+        NET_TRY(n, cudaMemcpyAsync(&newest, n->d_ring_cnt + ((clock - 1) % n->R), 4, cudaMemcpyDeviceToHost, st));
+        NET_TRY(n, cudaStreamSynchronize(st));
+    }
+    out->steps_done = clock;
+    out->events = s[0];
+    out->spikes = s[1] + newest;
+    out->graph_launches = n->graph_launches;
+    out->kernel_launches = n->kernel_launches;
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_get_state(szsnn_net* n, int slot, float* host)
+{
+    if (!n || slot < 0 || slot > 3 || !host) return SZSNN_ERR_ARG;
+    NET_TRY(n, cudaMemcpyAsync(host, n->d_st[slot], (size_t)n->U * 4, cudaMemcpyDeviceToHost, n->ctx->stream));
+    NET_TRY(n, cudaStreamSynchronize(n->ctx->stream));
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_set_state(szsnn_net* n, int slot, const float* host)
+{
+    if (!n || slot < 0 || slot > 3 || !host) return SZSNN_ERR_ARG;
+    NET_TRY(n, cudaMemcpyAsync(n->d_st[slot], host, (size_t)n->U * 4, cudaMemcpyHostToDevice, n->ctx->stream));
+    NET_TRY(n, cudaStreamSynchronize(n->ctx->stream));
+    return SZSNN_OK;
+}
+
+// checkpoint blob: header | 4 state slots | ring counts | ring ids | stats
+struct CkptHeader { uint64_t magic, U, D, clock; };
+static const uint64_t kCkptMagic = 0x535A534E4E434B31ull;  // "SZSNNCK1"
+
+extern "C" int szsnn_net_checkpoint_size(szsnn_net* n, uint64_t* bytes)
+{
+    if (!n || !bytes) return SZSNN_ERR_ARG;
+    *bytes = sizeof(CkptHeader) + (uint64_t)4 * n->U * 4 + (uint64_t)n->R * 4 + (uint64_t)n->R * n->U * 4 + 32;
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_checkpoint(szsnn_net* n, void* blob, uint64_t bytes)
+{
+    uint64_t need = 0;
+    if (szsnn_net_checkpoint_size(n, &need) || !blob || bytes < need) return n ? szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "checkpoint buffer too small") : SZSNN_ERR_ARG;
+    cudaStream_t st = n->ctx->stream;
+    char* p = (char*)blob;
+    CkptHeader h{kCkptMagic, (uint64_t)n->U, (uint64_t)n->D, 0};
+    NET_TRY(n, cudaMemcpyAsync(&h.clock, n->d_clock, 8, cudaMemcpyDeviceToHost, st));
+    char* q = p + sizeof(CkptHeader);
+    for (int k = 0; k < 4; ++k) {
+        NET_TRY(n, cudaMemcpyAsync(q, n->d_st[k], (size_t)n->U * 4, cudaMemcpyDeviceToHost, st));
+        q += (size_t)n->U * 4;
+    }
+    NET_TRY(n, cudaMemcpyAsync(q, n->d_ring_cnt, (size_t)n->R * 4, cudaMemcpyDeviceToHost, st));
+    q += (size_t)n->R * 4;
+    NET_TRY(n, cudaMemcpyAsync(q, n->d_ring_ids, (size_t)n->R * n->U * 4, cudaMemcpyDeviceToHost, st));
+    q += (size_t)n->R * n->U * 4;
+    NET_TRY(n, cudaMemcpyAsync(q, n->d_stats, 32, cudaMemcpyDeviceToHost, st));
+    NET_TRY(n, cudaStreamSynchronize(st));
+    std::memcpy(p, &h, sizeof(h));
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_restore(szsnn_net* n, const void* blob, uint64_t bytes)
+{
+    uint64_t need = 0;
+    if (szsnn_net_checkpoint_size(n, &need) || !blob || bytes < need) return n ? szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "checkpoint blob too small") : SZSNN_ERR_ARG;
+    const char* p = (const char*)blob;
+    CkptHeader h;
+    std::memcpy(&h, p, sizeof(h));
+    if (h.magic != kCkptMagic || h.U != (uint64_t)n->U || h.D != (uint64_t)n->D)
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "checkpoint does not match this network");
+    cudaStream_t st = n->ctx->stream;
+    const char* q = p + sizeof(CkptHeader);
+    for (int k = 0; k < 4; ++k) {
+        NET_TRY(n, cudaMemcpyAsync(n->d_st[k], q, (size_t)n->U * 4, cudaMemcpyHostToDevice, st));
+        q += (size_t)n->U * 4;
+    }
+    NET_TRY(n, cudaMemcpyAsync(n->d_ring_cnt, q, (size_t)n->R * 4, cudaMemcpyHostToDevice, st));
+    q += (size_t)n->R * 4;
+    NET_TRY(n, cudaMemcpyAsync(n->d_ring_ids, q, (size_t)n->R * n->U * 4, cudaMemcpyHostToDevice, st));
+    q += (size_t)n->R * n->U * 4;
+    NET_TRY(n, cudaMemcpyAsync(n->d_stats, q, 32, cudaMemcpyHostToDevice, st));
+    long long clock = (long long)h.clock;
+    NET_TRY(n, cudaMemcpyAsync(n->d_clock, &clock, 8, cudaMemcpyHostToDevice, st));
+    NET_TRY(n, cudaStreamSynchronize(st));
+    n->steps_done = clock;
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_get_synapses(szsnn_net* n, uint64_t* row_ptr, int32_t* tgt, float* w)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    cudaStream_t st = n->ctx->stream;
+    if (row_ptr)
+        NET_TRY(n, cudaMemcpyAsync(row_ptr, n->d_row_ptr, ((size_t)n->U * n->D + 1) * 8, cudaMemcpyDeviceToHost, st));
+    if ((tgt || w) && n->n_syn) {
+        int32_t* dt = nullptr;
+        float* dw = nullptr;
+        NET_TRY(n, dalloc(&dt, (size_t)n->n_syn));
+        NET_TRY(n, dalloc(&dw, (size_t)n->n_syn));
+        k_unpack_syn<<<1024, 256, 0, st>>>(n->d_syn, dt, dw, n->n_syn);
+        NET_TRY(n, cudaGetLastError());
+        if (tgt) NET_TRY(n, cudaMemcpyAsync(tgt, dt, (size_t)n->n_syn * 4, cudaMemcpyDeviceToHost, st));
+        if (w) NET_TRY(n, cudaMemcpyAsync(w, dw, (size_t)n->n_syn * 4, cudaMemcpyDeviceToHost, st));
+        NET_TRY(n, cudaStreamSynchronize(st));
+        cudaFree(dt);
+        cudaFree(dw);
+    }
+    NET_TRY(n, cudaStreamSynchronize(st));
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_check_finite(szsnn_net* n, int* finite_out)
+{
+    if (!n || !finite_out) return SZSNN_ERR_ARG;
+    cudaStream_t st = n->ctx->stream;
+    uint32_t* flag = nullptr;
+    NET_TRY(n, dalloc(&flag, 1));
+    NET_TRY(n, cudaMemsetAsync(flag, 0, 4, st));
+    for (int k = 0; k < 4; ++k) {
+        k_check_finite<<<512, 256, 0, st>>>(n->d_st[k], n->U, flag);
+        NET_TRY(n, cudaGetLastError());
+    }
+    uint32_t h = 0;
+    NET_TRY(n, cudaMemcpyAsync(&h, flag, 4, cudaMemcpyDeviceToHost, st));
+    NET_TRY(n, cudaStreamSynchronize(st));
+    cudaFree(flag);
+    *finite_out = h ? 0 : 1;
+    if (h) {
+        uint32_t code = SZSNN_DEV_NONFINITE, zero = 0;
+        // record as the sticky device error when none is set yet
+        uint32_t cur[2] = {0, 0};
+        NET_TRY(n, cudaMemcpy(cur, n->ctx->d_err, 8, cudaMemcpyDeviceToHost));
+        if (cur[0] == 0) {
+            NET_TRY(n, cudaMemcpy(n->ctx->d_err, &code, 4, cudaMemcpyHostToDevice));
+            NET_TRY(n, cudaMemcpy(n->ctx->d_err + 1, &zero, 4, cudaMemcpyHostToDevice));
+        }
+    }
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_last_inputs(szsnn_net* n, float* in_exc, float* in_inh)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    cudaStream_t st = n->ctx->stream;
+    if (in_exc && n->N) NET_TRY(n, cudaMemcpyAsync(in_exc, n->d_dbg_in, (size_t)n->N * 4, cudaMemcpyDeviceToHost, st));
+    if (in_inh && n->N)
+        NET_TRY(n, cudaMemcpyAsync(in_inh, n->d_dbg_in + std::max<int64_t>(n->N, 1), (size_t)n->N * 4, cudaMemcpyDeviceToHost, st));
+    NET_TRY(n, cudaStreamSynchronize(st));
+    return SZSNN_OK;
+}

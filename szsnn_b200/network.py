@@ -1,0 +1,229 @@
+"""Native network path: delay-bucketed CSR, device spike ring, CUDA graphs.
+
+A Network is the B200 form of Simulation + NetworkGraph for networks beyond
+the reference layout's limits (<= 64 delay steps, <= 256 partitions, bundles
+padded to 32 slots -- GroupData.cpp:94-228, scatter_kernel.cl:82,291).
+Units are neurons 0..N-1 followed by sources N..N+P-1; a spike emitted at
+step t over a synapse of delay m (m = user delay + 1, NetworkGraph.ipp:431)
+is integrated by the update of step t + m, exactly as the reference's
+scatter/gather double buffer delivers it (scatter_kernel.cl:154,207,325;
+gather_kernel.cl:55-58).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+
+
+@dataclass
+class Pop:
+    model: int
+    begin: int
+    end: int
+    params: np.ndarray = field(default_factory=lambda: np.zeros(12, np.float32))
+    per_unit: np.ndarray | None = None   # [12][end-begin] fp32, overrides params
+    seed: int = 0
+    flags: int = 0
+
+    def to_c(self, keep: list) -> L.PopDesc:
+        p = L.PopDesc()
+        p.model, p.flags, p.begin, p.end = self.model, self.flags, self.begin, self.end
+        pv = np.zeros(12, np.float32)
+        pv[: len(self.params)] = np.asarray(self.params, np.float32)
+        for i in range(12):
+            p.p[i] = float(pv[i])
+        if self.per_unit is not None:
+            a = np.zeros((12, self.end - self.begin), np.float32)
+            pu = np.asarray(self.per_unit, np.float32)
+            a[: pu.shape[0]] = pu
+            a = np.ascontiguousarray(a)
+            keep.append(a)
+            p.pn_host = a.ctypes.data
+        p.seed = self.seed
+        return p
+
+
+@dataclass
+class GenBlock:
+    """Fixed fan-out generator block (see szsnn_gen_block)."""
+    src_begin: int
+    src_count: int
+    tgt_begin: int
+    tgt_count: int
+    fanout: int
+    w_lo: float
+    w_hi: float
+    w_sign: float = 1.0
+    d_lo: int = 1
+    d_hi: int = 1
+    exclude_self: bool = False
+    stream: int = 0
+
+    def to_c(self, syn_offset: int) -> L.GenBlock:
+        return L.GenBlock(self.src_begin, self.src_count, self.tgt_begin, self.tgt_count, self.fanout,
+                          1 if self.exclude_self else 0, self.w_lo, self.w_hi, self.w_sign, self.d_lo, self.d_hi,
+                          self.stream, syn_offset)
+
+
+def csr_from_synapses(n_units: int, max_delay: int, src, tgt, w, delay):
+    """Bucket a synapse list into (row_ptr, tgt, w): rows by source, stably by delay."""
+    src = np.asarray(src, np.int64)
+    delay = np.asarray(delay, np.int64)
+    if len(src) and (delay.min() < 1 or delay.max() > max_delay):
+        raise ValueError("delays must be in 1..max_delay")
+    key = src * max_delay + (delay - 1)
+    order = np.argsort(key, kind="stable")
+    counts = np.bincount(key, minlength=n_units * max_delay) if len(src) else np.zeros(n_units * max_delay, np.int64)
+    row_ptr = np.zeros(n_units * max_delay + 1, np.uint64)
+    row_ptr[1:] = np.cumsum(counts, dtype=np.uint64)
+    return row_ptr, np.asarray(tgt, np.int32)[order].copy(), np.asarray(w, np.float32)[order].copy()
+
+
+class Network:
+    def __init__(self, ctx, n_neurons: int, n_sources: int, max_delay: int, pops: list[Pop], csr=None,
+                 state=None, acc_mode: int = L.ACC_FLOAT, graph_chunk: int = 100, n_synapses: int | None = None):
+        self.ctx = ctx
+        self.lib = L.lib()
+        self.N, self.P, self.D = int(n_neurons), int(n_sources), int(max_delay)
+        self.U = self.N + self.P
+        self.words = (self.U + 31) // 32
+        self.pops = pops
+        d = L.NetDesc()
+        d.n_neurons, d.n_sources, d.max_delay, d.n_pops = self.N, self.P, self.D, len(pops)
+        keep = []
+        for i, p in enumerate(pops):
+            d.pops[i] = p.to_c(keep)
+        if csr is not None:
+            rp, tg, ww = (np.ascontiguousarray(csr[0], np.uint64), np.ascontiguousarray(csr[1], np.int32),
+                          np.ascontiguousarray(csr[2], np.float32))
+            keep += [rp, tg, ww]
+            d.n_synapses = len(tg)
+            d.row_ptr_host, d.tgt_host, d.w_host = rp.ctypes.data, tg.ctypes.data, ww.ctypes.data
+        else:
+            d.n_synapses = int(n_synapses or 0)
+        if state is not None:
+            for k in range(4):
+                if state[k] is not None:
+                    a = np.ascontiguousarray(state[k], np.float32)
+                    if len(a) != self.U:
+                        raise ValueError("state slots must have n_neurons + n_sources entries")
+                    keep.append(a)
+                    d.state_host[k] = a.ctypes.data
+        d.acc_mode = acc_mode
+        d.graph_chunk = graph_chunk
+        h = C.c_void_p()
+        L.check(self.lib.szsnn_net_create(ctx.h, C.byref(d), C.byref(h)), ctx.h, "net_create")
+        self.h = h.value
+        self.n_synapses = int(d.n_synapses)
+
+    def generate(self, blocks: list[GenBlock], seed: int) -> None:
+        off = 0
+        arr = (L.GenBlock * max(len(blocks), 1))()
+        for i, b in enumerate(blocks):
+            arr[i] = b.to_c(off)
+            off += b.src_count * b.fanout
+        L.check(self.lib.szsnn_net_generate(self.h, arr, len(blocks), seed), self.ctx.h, "net_generate")
+        self.n_synapses = off
+
+    # Simulation::stepAndFired(fInput) (Simulation.ipp:517-530)
+    def step(self, forced_words=None, current=None, fired=True) -> np.ndarray | None:
+        fw = None if forced_words is None else np.ascontiguousarray(forced_words, np.uint32)
+        cu = None if current is None else np.ascontiguousarray(current, np.float32)
+        out = np.zeros(self.words, np.uint32) if fired else None
+        L.check(self.lib.szsnn_net_step(self.h, None if fw is None else fw.ctypes.data,
+                                        None if cu is None else cu.ctypes.data,
+                                        None if out is None else out.ctypes.data), self.ctx.h, "net_step")
+        return out
+
+    def run(self, steps: int, forced_words=None, raster=True) -> np.ndarray | None:
+        fw = None if forced_words is None else np.ascontiguousarray(forced_words, np.uint32)
+        out = np.zeros((steps, self.words), np.uint32) if raster else None
+        L.check(self.lib.szsnn_net_run(self.h, steps, None if fw is None else fw.ctypes.data,
+                                       None if out is None else out.ctypes.data), self.ctx.h, "net_run")
+        return out
+
+    def run_device(self, steps: int, forced_ptr=None, current_ptr=None, raster_ptr=None) -> None:
+        L.check(self.lib.szsnn_net_run_device(self.h, steps, forced_ptr, current_ptr, raster_ptr), self.ctx.h,
+                "net_run_device")
+
+    def profile(self, steps: int) -> tuple[float, float, float]:
+        p, u, t = C.c_double(), C.c_double(), C.c_double()
+        L.check(self.lib.szsnn_net_profile(self.h, steps, C.byref(p), C.byref(u), C.byref(t)), self.ctx.h, "profile")
+        return p.value, u.value, t.value
+
+    def set_tuning(self, group: int = 0, blocks: int = -1, update_block: int = 0) -> None:
+        L.check(self.lib.szsnn_net_set_tuning(self.h, group, blocks, update_block), self.ctx.h, "set_tuning")
+
+    def stats(self) -> dict:
+        s = L.NetStats()
+        L.check(self.lib.szsnn_net_stats_get(self.h, C.byref(s)), self.ctx.h, "stats")
+        return dict(steps_done=s.steps_done, events=s.events, spikes=s.spikes,
+                    graph_launches=s.graph_launches, kernel_launches=s.kernel_launches)
+
+    def get_state(self, slot: int) -> np.ndarray:
+        out = np.zeros(self.U, np.float32)
+        L.check(self.lib.szsnn_net_get_state(self.h, slot, out.ctypes.data), self.ctx.h, "get_state")
+        return out
+
+    def set_state(self, slot: int, values) -> None:
+        a = np.ascontiguousarray(values, np.float32)
+        if len(a) != self.U:
+            raise ValueError("state slot length must be n_neurons + n_sources")
+        L.check(self.lib.szsnn_net_set_state(self.h, slot, a.ctypes.data), self.ctx.h, "set_state")
+
+    def checkpoint(self) -> bytes:
+        n = C.c_uint64()
+        L.check(self.lib.szsnn_net_checkpoint_size(self.h, C.byref(n)), self.ctx.h)
+        buf = np.zeros(n.value, np.uint8)
+        L.check(self.lib.szsnn_net_checkpoint(self.h, buf.ctypes.data, n.value), self.ctx.h, "checkpoint")
+        return buf.tobytes()
+
+    def restore(self, blob: bytes) -> None:
+        a = np.frombuffer(blob, np.uint8).copy()
+        L.check(self.lib.szsnn_net_restore(self.h, a.ctypes.data, len(a)), self.ctx.h, "restore")
+
+    def synapses(self):
+        rp = np.zeros(self.U * self.D + 1, np.uint64)
+        tg = np.zeros(self.n_synapses, np.int32)
+        ww = np.zeros(self.n_synapses, np.float32)
+        L.check(self.lib.szsnn_net_get_synapses(self.h, rp.ctypes.data, tg.ctypes.data, ww.ctypes.data),
+                self.ctx.h, "get_synapses")
+        return rp, tg, ww
+
+    def last_inputs(self):
+        e = np.zeros(self.N, np.float32)
+        i = np.zeros(self.N, np.float32)
+        L.check(self.lib.szsnn_net_last_inputs(self.h, e.ctypes.data, i.ctypes.data), self.ctx.h)
+        return e, i
+
+    def check_finite(self) -> bool:
+        f = C.c_int()
+        L.check(self.lib.szsnn_net_check_finite(self.h, C.byref(f)), self.ctx.h)
+        return bool(f.value)
+
+    def close(self) -> None:
+        if getattr(self, "h", None) is not None and self.ctx.h is not None:
+            self.lib.szsnn_net_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def words_to_ids(words: np.ndarray, n_units: int) -> np.ndarray:
+    bits = np.unpackbits(np.ascontiguousarray(words, np.uint32).view(np.uint8), bitorder="little")
+    return np.nonzero(bits[:n_units])[0]
+
+
+def ids_to_words(ids, n_units: int) -> np.ndarray:
+    w = np.zeros((n_units + 31) // 32, np.uint32)
+    ids = np.asarray(ids, np.int64)
+    np.bitwise_or.at(w, ids // 32, (np.uint32(1) << (ids % 32).astype(np.uint32)))
+    return w
