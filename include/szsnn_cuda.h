@@ -214,7 +214,7 @@ enum {
     SZSNN_POISSON     = 3,
     SZSNN_CONST_RATE  = 4
 };
-#define SZSNN_MAX_POPS 16
+#define SZSNN_MAX_POPS 65536
 #define SZSNN_POP_IZH_HALF_STEPS 1u
 
 /* Parameter slots: IF_curr_exp 0 v_rest 1 cm 2 tau_m 3 tau_refrac 4 tau_syn_E
@@ -239,8 +239,8 @@ typedef struct {
 typedef struct {
     int64_t  n_neurons, n_sources;
     int32_t  max_delay;             /* D, 1..1024 */
-    int32_t  n_pops;
-    szsnn_pop_desc pops[SZSNN_MAX_POPS];
+    int32_t  n_pops;                /* <= SZSNN_MAX_POPS */
+    const szsnn_pop_desc* pops;     /* ranges disjoint, sorted by begin */
     uint64_t n_synapses;
     const uint64_t* row_ptr_host;   /* (N+P)*D+1, or NULL with szsnn_net_generate */
     const int32_t*  tgt_host;
@@ -248,7 +248,9 @@ typedef struct {
     const float*    state_host[4];  /* initial state slots (length N+P) or NULL = 0 */
     uint32_t acc_mode;
     uint32_t graph_chunk;           /* steps per captured CUDA graph (0 = 100) */
-    int64_t  raster_capacity;       /* device raster ring, steps (0 = graph_chunk) */
+    int64_t  raster_capacity;       /* reserved, 0 */
+    const int32_t* group_host;      /* per-unit group id (e.g. the network of a batch), or NULL */
+    int32_t  n_groups;              /* spike counters kept per group when group_host is set */
 } szsnn_net_desc;
 
 /* Fixed fan-out generator block (device-side; identical algorithm in the
@@ -290,6 +292,8 @@ int szsnn_net_run(szsnn_net* net, int64_t steps, const uint32_t* forced_host,
 int szsnn_net_run_device(szsnn_net* net, int64_t steps, const uint32_t* forced_dev,
                          const float* current_dev, uint32_t* raster_dev);
 int szsnn_net_stats_get(szsnn_net* net, szsnn_net_stats* out);
+/* spikes per group since creation (or the last reset): counts[n_groups] */
+int szsnn_net_group_spikes(szsnn_net* net, uint64_t* counts, int reset);
 /* state slot k (length N+P) copy out / in (checkpoint) */
 int szsnn_net_get_state(szsnn_net* net, int slot, float* host);
 int szsnn_net_set_state(szsnn_net* net, int slot, const float* host);
@@ -304,8 +308,8 @@ int szsnn_net_check_finite(szsnn_net* net, int* finite_out);
 /* inputs integrated at the last step (debug/parity): in_exc, in_inh (N) */
 int szsnn_net_last_inputs(szsnn_net* net, float* in_exc, float* in_inh);
 
-/* per-kernel device time of `steps` directly launched steps (CUDA events around
- * each kernel on the launching stream), summed over the steps, in ms */
+/* per-kernel device time of `steps` steps run as one CUDA graph with event
+ * records between the kernels, summed over the steps, in ms */
 int szsnn_net_profile(szsnn_net* net, int64_t steps, double* propagate_ms, double* update_ms, double* total_ms);
 /* total_ms: device time (CUDA events on the stream) of the last szsnn_net_run /
  * szsnn_net_run_device; propagate/update: the last szsnn_net_profile */

@@ -15,7 +15,7 @@ SZSNN_OK = 0
 ERR_NAMES = {1: "ARG", 2: "CUDA", 3: "NOMEM", 4: "LIMIT", 5: "DEVICE", 6: "TIMEOUT", 7: "STATE"}
 
 IF_CURR_EXP, IF_COND_EXP, IZHIKEVICH, POISSON, CONST_RATE = 0, 1, 2, 3, 4
-MAX_POPS = 16
+MAX_POPS = 65536
 POP_IZH_HALF_STEPS = 1
 ACC_FLOAT, ACC_FIXED = 0, 1
 
@@ -62,10 +62,10 @@ class PopDesc(C.Structure):
 
 class NetDesc(C.Structure):
     _fields_ = [("n_neurons", C.c_int64), ("n_sources", C.c_int64), ("max_delay", C.c_int32),
-                ("n_pops", C.c_int32), ("pops", PopDesc * MAX_POPS), ("n_synapses", C.c_uint64),
+                ("n_pops", C.c_int32), ("pops", C.c_void_p), ("n_synapses", C.c_uint64),
                 ("row_ptr_host", C.c_void_p), ("tgt_host", C.c_void_p), ("w_host", C.c_void_p),
                 ("state_host", C.c_void_p * 4), ("acc_mode", C.c_uint32), ("graph_chunk", C.c_uint32),
-                ("raster_capacity", C.c_int64)]
+                ("raster_capacity", C.c_int64), ("group_host", C.c_void_p), ("n_groups", C.c_int32)]
 
 
 class GenBlock(C.Structure):
@@ -116,6 +116,7 @@ SIGNATURES = {
     "szsnn_net_run": (_I, [_P, _I64, _P, _P]),
     "szsnn_net_run_device": (_I, [_P, _I64, _P, _P, _P]),
     "szsnn_net_stats_get": (_I, [_P, _P]),
+    "szsnn_net_group_spikes": (_I, [_P, _P, _I]),
     "szsnn_net_get_state": (_I, [_P, _I, _P]),
     "szsnn_net_set_state": (_I, [_P, _I, _P]),
     "szsnn_net_checkpoint_size": (_I, [_P, C.POINTER(C.c_uint64)]),

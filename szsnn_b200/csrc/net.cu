@@ -59,6 +59,8 @@ struct NetDev {
     uint32_t* err;
     float* dbg_in_e;
     float* dbg_in_i;
+    const int32_t* group;                  // per-unit group or null
+    unsigned long long* group_spikes;      // [n_groups]
 };
 
 struct szsnn_net {
@@ -67,9 +69,12 @@ struct szsnn_net {
     int32_t D = 0, R = 0;
     uint32_t acc_mode = 0;
     int32_t npops = 0;
-    szsnn_pop_desc pops[SZSNN_MAX_POPS];
+    std::vector<szsnn_pop_desc> pops;
     PopDev* d_pops = nullptr;
-    float* d_pn[SZSNN_MAX_POPS] = {};
+    float* d_pn = nullptr;                 // all per-unit parameter arrays, back to back
+    int32_t* d_group = nullptr;
+    unsigned long long* d_group_spikes = nullptr;
+    int32_t n_groups = 0;
     uint64_t n_syn = 0;
     unsigned long long* d_row_ptr = nullptr;
     int2* d_syn = nullptr;
@@ -196,10 +201,12 @@ __global__ void __launch_bounds__(256) k_update(NetDev nd, int k_off, const uint
     const uint32_t lane = threadIdx.x & 31;
     bool spk = false;
     if (id < nd.U) {
-        int pi = -1;
-        for (int i = 0; i < nd.npops; ++i) {
-            if (id >= nd.pops[i].begin && id < nd.pops[i].end) { pi = i; break; }
+        int pi = -1;  // last population with begin <= id (ranges sorted, disjoint)
+        for (int lo = 0, hi = nd.npops - 1; lo <= hi;) {
+            const int mid = (lo + hi) >> 1;
+            if (nd.pops[mid].begin <= id) { pi = mid; lo = mid + 1; } else hi = mid - 1;
         }
+        if (pi >= 0 && id >= nd.pops[pi].end) pi = -1;
         if (pi >= 0) {
             const PopDev* pd = &nd.pops[pi];
             PopParams p{pd, id - pd->begin, pd->end - pd->begin};
@@ -241,6 +248,7 @@ __global__ void __launch_bounds__(256) k_update(NetDev nd, int k_off, const uint
             }
         }
     }
+    if (spk && nd.group) atomicAdd(&nd.group_spikes[nd.group[id]], 1ull);
     const uint32_t ball = __ballot_sync(0xffffffffu, spk);
     const int64_t wd = id >> 5;
     if (lane == 0 && out_words && wd < nd.words) out_words[wd] = ball;
@@ -383,6 +391,7 @@ NetDev make_dev(szsnn_net* n)
     d.acc_mode = n->acc_mode; d.ring_cnt = n->d_ring_cnt; d.ring_ids = n->d_ring_ids;
     d.clock = n->d_clock; d.stats = n->d_stats; d.err = n->ctx->d_err;
     d.dbg_in_e = nullptr; d.dbg_in_i = nullptr;
+    d.group = n->d_group; d.group_spikes = n->d_group_spikes;
     return d;
 }
 
@@ -422,7 +431,9 @@ void free_net(szsnn_net* n)
     for (auto& kv : n->graphs) cudaGraphExecDestroy(kv.second);
     n->graphs.clear();
     cudaFree(n->d_pops);
-    for (int i = 0; i < SZSNN_MAX_POPS; ++i) cudaFree(n->d_pn[i]);
+    cudaFree(n->d_pn);
+    cudaFree(n->d_group);
+    cudaFree(n->d_group_spikes);
     cudaFree(n->d_row_ptr);
     cudaFree(n->d_syn);
     for (int k = 0; k < 4; ++k) cudaFree(n->d_st[k]);
@@ -465,8 +476,10 @@ extern "C" int szsnn_net_create(szsnn_ctx* ctx, const szsnn_net_desc* d, szsnn_n
         return szsnn_set_error(ctx, SZSNN_ERR_LIMIT, "szsnn_net_create: more than 2^31-1 units");
     if (d->max_delay < 1 || d->max_delay > 1024)
         return szsnn_set_error(ctx, SZSNN_ERR_ARG, "szsnn_net_create: max_delay outside 1..1024");
-    if (d->n_pops < 0 || d->n_pops > SZSNN_MAX_POPS)
-        return szsnn_set_error(ctx, SZSNN_ERR_ARG, "szsnn_net_create: n_pops outside 0..16");
+    if (d->n_pops < 0 || d->n_pops > SZSNN_MAX_POPS || (d->n_pops > 0 && !d->pops))
+        return szsnn_set_error(ctx, SZSNN_ERR_ARG, "szsnn_net_create: bad population table");
+    if (d->group_host && (d->n_groups < 1))
+        return szsnn_set_error(ctx, SZSNN_ERR_ARG, "szsnn_net_create: group_host needs n_groups >= 1");
     if (d->acc_mode > 1) return szsnn_set_error(ctx, SZSNN_ERR_ARG, "szsnn_net_create: bad acc_mode");
     const int64_t N = d->n_neurons, U = d->n_neurons + d->n_sources;
     for (int i = 0; i < d->n_pops; ++i) {
@@ -481,9 +494,9 @@ extern "C" int szsnn_net_create(szsnn_ctx* ctx, const szsnn_net_desc* d, szsnn_n
             return szsnn_set_error(ctx, SZSNN_ERR_ARG, "pop " + std::to_string(i) + ": neuron model on source ids");
         if (p.begin < p.end && source_model && p.begin < N)
             return szsnn_set_error(ctx, SZSNN_ERR_ARG, "pop " + std::to_string(i) + ": source model on neuron ids");
-        for (int j = 0; j < i; ++j)
-            if (p.begin < d->pops[j].end && d->pops[j].begin < p.end)
-                return szsnn_set_error(ctx, SZSNN_ERR_ARG, "pops " + std::to_string(j) + " and " + std::to_string(i) + " overlap");
+        if (i > 0 && p.begin < d->pops[i - 1].end)
+            return szsnn_set_error(ctx, SZSNN_ERR_ARG,
+                                   "pops " + std::to_string(i - 1) + " and " + std::to_string(i) + " overlap or are not sorted");
     }
     const int D = d->max_delay;
     if (d->row_ptr_host) {  // host CSR: bucket pointers must be monotone and end at n_synapses
@@ -503,26 +516,47 @@ extern "C" int szsnn_net_create(szsnn_ctx* ctx, const szsnn_net_desc* d, szsnn_n
     n->acc_mode = d->acc_mode; n->npops = d->n_pops;
     n->chunk = d->graph_chunk ? (int)d->graph_chunk : 100;
     n->n_syn = d->n_synapses;
-    std::memcpy(n->pops, d->pops, sizeof(n->pops));
+    n->pops.assign(d->pops, d->pops + d->n_pops);
     cudaStream_t st = ctx->stream;
 #define C(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { std::string m_ = std::string(#x) + ": " + cudaGetErrorString(e_); int code_ = e_ == cudaErrorMemoryAllocation ? SZSNN_ERR_NOMEM : SZSNN_ERR_CUDA; free_net(n); return szsnn_set_error(ctx, code_, m_); } } while (0)
-    // populations
-    PopDev hp[SZSNN_MAX_POPS];
-    std::memset(hp, 0, sizeof(hp));
-    for (int i = 0; i < d->n_pops; ++i) {
-        const szsnn_pop_desc& p = d->pops[i];
-        hp[i].model = p.model; hp[i].flags = p.flags; hp[i].begin = p.begin; hp[i].end = p.end;
-        std::memcpy(hp[i].p, p.p, sizeof(hp[i].p));
-        hp[i].seed = p.seed;
-        if (p.pn_host && p.end > p.begin) {
-            size_t cnt = (size_t)12 * (p.end - p.begin);
-            C(dalloc(&n->d_pn[i], cnt));
-            C(cudaMemcpyAsync(n->d_pn[i], p.pn_host, cnt * sizeof(float), cudaMemcpyHostToDevice, st));
-            hp[i].pn = n->d_pn[i];
+    // populations; per-unit parameter arrays packed into one device buffer
+    {
+        std::vector<PopDev> hp((size_t)std::max(d->n_pops, 1));
+        size_t pn_total = 0;
+        for (int i = 0; i < d->n_pops; ++i)
+            if (d->pops[i].pn_host && d->pops[i].end > d->pops[i].begin) pn_total += (size_t)12 * (d->pops[i].end - d->pops[i].begin);
+        if (pn_total) C(dalloc(&n->d_pn, pn_total));
+        size_t off = 0;
+        for (int i = 0; i < d->n_pops; ++i) {
+            const szsnn_pop_desc& p = d->pops[i];
+            PopDev& q = hp[(size_t)i];
+            std::memset(&q, 0, sizeof(q));
+            q.model = p.model; q.flags = p.flags; q.begin = p.begin; q.end = p.end;
+            std::memcpy(q.p, p.p, sizeof(q.p));
+            q.seed = p.seed;
+            if (p.pn_host && p.end > p.begin) {
+                size_t cnt = (size_t)12 * (p.end - p.begin);
+                C(cudaMemcpyAsync(n->d_pn + off, p.pn_host, cnt * sizeof(float), cudaMemcpyHostToDevice, st));
+                q.pn = n->d_pn + off;
+                off += cnt;
+            }
         }
+        C(dalloc(&n->d_pops, hp.size()));
+        C(cudaMemcpyAsync(n->d_pops, hp.data(), hp.size() * sizeof(PopDev), cudaMemcpyHostToDevice, st));
+        C(cudaStreamSynchronize(st));
     }
-    C(dalloc(&n->d_pops, SZSNN_MAX_POPS));
-    C(cudaMemcpyAsync(n->d_pops, hp, sizeof(hp), cudaMemcpyHostToDevice, st));
+    if (d->group_host) {
+        for (int64_t i = 0; i < U; ++i)
+            if (d->group_host[i] < 0 || d->group_host[i] >= d->n_groups) {
+                free_net(n);
+                return szsnn_set_error(ctx, SZSNN_ERR_ARG, "group id outside 0..n_groups-1");
+            }
+        n->n_groups = d->n_groups;
+        C(dalloc(&n->d_group, (size_t)U));
+        C(cudaMemcpyAsync(n->d_group, d->group_host, (size_t)U * 4, cudaMemcpyHostToDevice, st));
+        C(dalloc(&n->d_group_spikes, (size_t)d->n_groups));
+        C(cudaMemsetAsync(n->d_group_spikes, 0, (size_t)d->n_groups * 8, st));
+    }
     // synapses
     C(dalloc(&n->d_row_ptr, (size_t)U * D + 1));
     C(dalloc(&n->d_syn, (size_t)n->n_syn));
@@ -769,26 +803,46 @@ extern "C" int szsnn_net_run_device(szsnn_net* n, int64_t steps, const uint32_t*
     return net_run_impl(n, steps, forced_dev, current_dev, raster_dev, false);
 }
 
-// Per-kernel device time: `steps` steps launched directly (no graph), with
-// CUDA events on the launching stream around every kernel.
+// Per-kernel device time: `steps` steps captured in one CUDA graph with an
+// event-record node after every kernel, so consecutive nodes run back to back
+// and each interval is one kernel's device time (no host launch gaps).
 extern "C" int szsnn_net_profile(szsnn_net* n, int64_t steps, double* prop_ms, double* upd_ms, double* total_ms)
 {
-    if (!n || steps < 1) return SZSNN_ERR_ARG;
+    if (!n || steps < 1 || steps > 100000) return SZSNN_ERR_ARG;
     cudaStream_t st = n->ctx->stream;
     NetDev d = make_dev(n);
     std::vector<cudaEvent_t> ev((size_t)(2 * steps + 1));
     for (auto& e : ev) NET_TRY(n, cudaEventCreate(&e));
-    NET_TRY(n, cudaEventRecord(ev[0], st));
-    for (int64_t k = 0; k < steps; ++k) {
-        NET_TRY(n, launch_propagate(n, d, 0));
-        NET_TRY(n, cudaEventRecord(ev[(size_t)(2 * k + 1)], st));
-        NET_TRY(n, launch_update(n, d, 0, nullptr, nullptr, nullptr));
-        k_advance<<<1, 1, 0, st>>>(n->d_clock, 1);
-        NET_TRY(n, cudaEventRecord(ev[(size_t)(2 * k + 2)], st));
-        n->steps_done += 1;
-        n->kernel_launches += 3;
+    cudaGraph_t g = nullptr;
+    NET_TRY(n, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal);
+    for (int64_t k = 0; k < steps && e == cudaSuccess; ++k) {
+        e = launch_propagate(n, d, (int)k);
+        if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[(size_t)(2 * k + 1)], st, cudaEventRecordExternal);
+        if (e == cudaSuccess) e = launch_update(n, d, (int)k, nullptr, nullptr, nullptr);
+        if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[(size_t)(2 * k + 2)], st, cudaEventRecordExternal);
     }
-    NET_TRY(n, cudaEventSynchronize(ev.back()));
+    if (e == cudaSuccess) {
+        k_advance<<<1, 1, 0, st>>>(n->d_clock, (int)steps);
+        e = cudaGetLastError();
+    }
+    cudaError_t e2 = cudaStreamEndCapture(st, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        for (auto& x : ev) cudaEventDestroy(x);
+        return szsnn_set_error(n->ctx, SZSNN_ERR_CUDA,
+                               std::string("profile capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    NET_TRY(n, e);
+    NET_TRY(n, cudaGraphLaunch(ex, st));
+    NET_TRY(n, cudaStreamSynchronize(st));
+    cudaGraphExecDestroy(ex);
+    n->steps_done += steps;
+    n->kernel_launches += (uint64_t)2 * steps + 1;
+    n->graph_launches += 1;
     double p = 0, u = 0;
     for (int64_t k = 0; k < steps; ++k) {
         float a = 0, b = 0;
@@ -799,7 +853,7 @@ extern "C" int szsnn_net_profile(szsnn_net* n, int64_t steps, double* prop_ms, d
     }
     float tot = 0;
     cudaEventElapsedTime(&tot, ev[0], ev.back());
-    for (auto& e : ev) cudaEventDestroy(e);
+    for (auto& x : ev) cudaEventDestroy(x);
     n->t_prop_ms = p;
     n->t_upd_ms = u;
     if (prop_ms) *prop_ms = p;
@@ -857,6 +911,16 @@ extern "C" int szsnn_net_stats_get(szsnn_net* n, szsnn_net_stats* out)
     out->spikes = s[1] + newest;
     out->graph_launches = n->graph_launches;
     out->kernel_launches = n->kernel_launches;
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_group_spikes(szsnn_net* n, uint64_t* counts, int reset)
+{
+    if (!n || !counts || !n->d_group_spikes) return n ? szsnn_set_error(n->ctx, SZSNN_ERR_STATE, "network has no groups") : SZSNN_ERR_ARG;
+    cudaStream_t st = n->ctx->stream;
+    NET_TRY(n, cudaMemcpyAsync(counts, n->d_group_spikes, (size_t)n->n_groups * 8, cudaMemcpyDeviceToHost, st));
+    if (reset) NET_TRY(n, cudaMemsetAsync(n->d_group_spikes, 0, (size_t)n->n_groups * 8, st));
+    NET_TRY(n, cudaStreamSynchronize(st));
     return SZSNN_OK;
 }
 

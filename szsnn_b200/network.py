@@ -85,7 +85,8 @@ def csr_from_synapses(n_units: int, max_delay: int, src, tgt, w, delay):
 
 class Network:
     def __init__(self, ctx, n_neurons: int, n_sources: int, max_delay: int, pops: list[Pop], csr=None,
-                 state=None, acc_mode: int = L.ACC_FLOAT, graph_chunk: int = 100, n_synapses: int | None = None):
+                 state=None, acc_mode: int = L.ACC_FLOAT, graph_chunk: int = 100, n_synapses: int | None = None,
+                 groups=None, n_groups: int = 0):
         self.ctx = ctx
         self.lib = L.lib()
         self.N, self.P, self.D = int(n_neurons), int(n_sources), int(max_delay)
@@ -95,8 +96,19 @@ class Network:
         d = L.NetDesc()
         d.n_neurons, d.n_sources, d.max_delay, d.n_pops = self.N, self.P, self.D, len(pops)
         keep = []
+        pop_arr = (L.PopDesc * max(len(pops), 1))()
         for i, p in enumerate(pops):
-            d.pops[i] = p.to_c(keep)
+            pop_arr[i] = p.to_c(keep)
+        keep.append(pop_arr)
+        d.pops = C.cast(pop_arr, C.c_void_p)
+        if groups is not None:
+            g = np.ascontiguousarray(groups, np.int32)
+            if len(g) != self.U:
+                raise ValueError("groups must have one entry per unit")
+            keep.append(g)
+            d.group_host = g.ctypes.data
+            d.n_groups = int(n_groups or (g.max() + 1))
+        self.n_groups = int(d.n_groups)
         if csr is not None:
             rp, tg, ww = (np.ascontiguousarray(csr[0], np.uint64), np.ascontiguousarray(csr[1], np.int32),
                           np.ascontiguousarray(csr[2], np.float32))
@@ -163,6 +175,12 @@ class Network:
         L.check(self.lib.szsnn_net_stats_get(self.h, C.byref(s)), self.ctx.h, "stats")
         return dict(steps_done=s.steps_done, events=s.events, spikes=s.spikes,
                     graph_launches=s.graph_launches, kernel_launches=s.kernel_launches)
+
+    def group_spikes(self, reset: bool = False) -> np.ndarray:
+        out = np.zeros(self.n_groups, np.uint64)
+        L.check(self.lib.szsnn_net_group_spikes(self.h, out.ctypes.data, 1 if reset else 0), self.ctx.h,
+                "group_spikes")
+        return out
 
     def get_state(self, slot: int) -> np.ndarray:
         out = np.zeros(self.U, np.float32)
