@@ -308,13 +308,19 @@ int szsnn_net_check_finite(szsnn_net* net, int* finite_out);
 /* inputs integrated at the last step (debug/parity): in_exc, in_inh (N) */
 int szsnn_net_last_inputs(szsnn_net* net, float* in_exc, float* in_inh);
 
-/* per-kernel device time of `steps` steps run as one CUDA graph with event
- * records between the kernels, summed over the steps, in ms */
-int szsnn_net_profile(szsnn_net* net, int64_t steps, double* propagate_ms, double* update_ms, double* total_ms);
+/* per-kernel device time: `steps` replays of the current step's propagate and
+ * update launches on scratch copies of the state (the network is unchanged),
+ * timed with CUDA events on the stream; sums over the replays, in ms, and the
+ * synaptic events one propagate launch delivers */
+int szsnn_net_profile(szsnn_net* net, int64_t steps, double* propagate_ms, double* update_ms,
+                      double* events_per_launch);
 /* total_ms: device time (CUDA events on the stream) of the last szsnn_net_run /
  * szsnn_net_run_device; propagate/update: the last szsnn_net_profile */
 int szsnn_net_timing(szsnn_net* net, double* propagate_ms, double* update_ms, double* total_ms);
-int szsnn_net_set_tuning(szsnn_net* net, int propagate_group, int propagate_blocks, int update_block);
+/* launch shapes: propagate mode 0 = `group` lanes per (delay, spike) bucket
+ * segment (4/8/16/32), mode 1 = warp-flattened walk over `group` items per
+ * warp (8/16/32); propagate grid blocks (0 = 16 per SM); update block size */
+int szsnn_net_set_tuning(szsnn_net* net, int propagate_mode, int group, int propagate_blocks, int update_block);
 
 #ifdef __cplusplus
 }

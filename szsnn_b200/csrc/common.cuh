@@ -106,13 +106,15 @@ __device__ __forceinline__ bool sz_poisson_fires(uint64_t seed, int64_t id, int6
 // ---------------------------------------------------------------- models
 // IF_curr_exp -- IF_curr_exp_update_kernel.cl:230-287.
 // p: 0 v_rest 1 cm 2 tau_m 3 tau_refrac 4 tau_syn_E 5 tau_syn_I 6 i_offset 7 v_reset 8 v_thresh
+// de, di: (1 - 1/tau_syn_E), (1 - 1/tau_syn_I), the same fp32 operations
+// whether evaluated per step (reference layout) or once per population.
 template <class P>
 __device__ __forceinline__ bool sz_if_curr_exp(const P& p, float& v, float& ie, float& ii, float& fired,
-                                               float in_e, float in_i, float i_ext, bool forced)
+                                               float in_e, float in_i, float i_ext, bool forced, float de, float di)
 {
     const float one = 1.0f;
-    float Ie = ((one - one / p(4)) * ie) + in_e;
-    float Ii = ((one - one / p(5)) * ii) + in_i;
+    float Ie = (de * ie) + in_e;
+    float Ii = (di * ii) + in_i;
     float I = ((Ie + Ii) + i_ext) + p(6);
     ie = Ie;
     ii = Ii;
@@ -135,11 +137,11 @@ __device__ __forceinline__ bool sz_if_curr_exp(const P& p, float& v, float& ie, 
 // then v integrates with the new conductances.  p: IF_curr_exp slots + 9 e_rev_E 10 e_rev_I
 template <class P>
 __device__ __forceinline__ bool sz_if_cond_exp(const P& p, float& v, float& ge, float& gi, float& fired,
-                                               float in_e, float in_i, float i_ext, bool forced)
+                                               float in_e, float in_i, float i_ext, bool forced, float de, float di)
 {
     const float one = 1.0f;
-    float g_e = ((one - one / p(4)) * ge) + in_e;
-    float g_i = ((one - one / p(5)) * gi) - in_i;
+    float g_e = (de * ge) + in_e;
+    float g_i = (di * gi) - in_i;
     ge = g_e;
     gi = g_i;
     bool refr = fired <= p(3);
@@ -192,5 +194,8 @@ __device__ __forceinline__ bool sz_const_rate(const P& p, float& last, bool forc
     last = l;
     return spk;
 }
+
+// 1 - 1/tau in fp32 (IF_curr_exp_update_kernel.cl:230-231)
+__host__ __device__ __forceinline__ float sz_decay(float tau) { return 1.0f - 1.0f / tau; }
 
 __host__ __device__ __forceinline__ int64_t sz_div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }

@@ -28,12 +28,15 @@
 #include <map>
 #include <tuple>
 
+// slots 0..11 as szsnn_pop_desc; 12, 13 = 1 - 1/tau_syn_E, 1 - 1/tau_syn_I
+// (IF models), computed once on the host with the same fp32 operations
+#define POP_SLOTS 16
 struct PopDev {
     int32_t model;
     uint32_t flags;
     int64_t begin, end;
-    float p[12];
-    const float* pn;
+    float p[POP_SLOTS];
+    const float* pn;   // per-unit parameters [POP_SLOTS][end-begin], or null
     uint64_t seed;
 };
 
@@ -61,6 +64,7 @@ struct NetDev {
     float* dbg_in_i;
     const int32_t* group;                  // per-unit group or null
     unsigned long long* group_spikes;      // [n_groups]
+    const int2* blk_pop;                   // per update block: (first overlapping pop, count)
 };
 
 struct szsnn_net {
@@ -75,6 +79,7 @@ struct szsnn_net {
     int32_t* d_group = nullptr;
     unsigned long long* d_group_spikes = nullptr;
     int32_t n_groups = 0;
+    int2* d_blk_pop = nullptr;             // sized for 32-thread blocks, filled for upd_block
     uint64_t n_syn = 0;
     unsigned long long* d_row_ptr = nullptr;
     int2* d_syn = nullptr;
@@ -96,7 +101,7 @@ struct szsnn_net {
     std::map<std::tuple<int, int>, cudaGraphExec_t> graphs;
     int64_t steps_done = 0;
     uint64_t graph_launches = 0, kernel_launches = 0;
-    int prop_group = 16, prop_blocks = 0, upd_block = 256;
+    int prop_mode = 0, prop_group = 16, prop_blocks = 0, upd_block = 256;
     double t_prop_ms = 0, t_upd_ms = 0, t_total_ms = 0;
     cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;  // around the last szsnn_net_run*
     bool run_timed = false;
@@ -104,14 +109,27 @@ struct szsnn_net {
 
 namespace {
 
-struct PopParams {
-    const PopDev* pd;
+struct UnitParams {  // per-unit parameter arrays
+    const float* pn;
     int64_t off, cnt;
-    __device__ __forceinline__ float operator()(int k) const
-    {
-        return pd->pn ? pd->pn[(int64_t)k * cnt + off] : pd->p[k];
-    }
+    __device__ __forceinline__ float operator()(int k) const { return pn[(int64_t)k * cnt + off]; }
 };
+struct SharedParams {  // one parameter set for the population (staged in shared memory)
+    const float* p;
+    __device__ __forceinline__ float operator()(int k) const { return p[k]; }
+};
+
+// neuron update for one unit; returns the spike
+template <class P>
+__device__ __forceinline__ bool run_neuron(const P& p, int model, uint32_t flags, float& v, float& g1, float& g2,
+                                           float& fr, float in_e, float in_i, float i_ext, bool f)
+{
+    if (model == SZSNN_IF_CURR_EXP) return sz_if_curr_exp(p, v, g1, g2, fr, in_e, in_i, i_ext, f, p(12), p(13));
+    if (model == SZSNN_IF_COND_EXP) return sz_if_cond_exp(p, v, g1, g2, fr, in_e, in_i, i_ext, f, p(12), p(13));
+    if (model == SZSNN_IZHIKEVICH)
+        return sz_izhikevich(p, v, g1, in_e, in_i, i_ext, f, (flags & SZSNN_POP_IZH_HALF_STEPS) != 0);
+    return false;
+}
 
 __global__ void k_advance(long long* clock, int k) { *clock += k; }
 
@@ -193,59 +211,217 @@ __global__ void __launch_bounds__(256) k_propagate(NetDev nd, int k_off)
     if (threadIdx.x == 0 && s_ev) atomicAdd(&nd.stats[0], s_ev);
 }
 
-__global__ void __launch_bounds__(256) k_update(NetDev nd, int k_off, const uint32_t* forced, const float* current,
-                                                uint32_t* out_words)
+// Warp-flattened delivery: lanes 0..IPW-1 each resolve one (delay, spike)
+// work item to its bucket segment; the warp then walks the concatenation of
+// those segments 32 synapses at a time (owner segment found by a binary
+// search over the lanes' exclusive offsets with shuffles), UNR loads in
+// flight per lane before their atomics.
+template <int IPW>
+__global__ void __launch_bounds__(256) k_propagate_flat(NetDev nd, int k_off)
 {
+    constexpr int UNR = 4;
+    __shared__ uint32_t s_pre[1025];
+    __shared__ unsigned long long s_ev;
     const long long t = *nd.clock + k_off;
-    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int D = nd.D, R = D + 1;
+    for (int m = threadIdx.x + 1; m <= D; m += blockDim.x) {
+        long long tm = t - m;
+        s_pre[m] = (tm >= 0) ? nd.ring_cnt[tm % R] : 0u;
+    }
+    if (threadIdx.x == 0) { s_pre[0] = 0; s_ev = 0; }
+    __syncthreads();
     const uint32_t lane = threadIdx.x & 31;
-    bool spk = false;
-    if (id < nd.U) {
-        int pi = -1;  // last population with begin <= id (ranges sorted, disjoint)
-        for (int lo = 0, hi = nd.npops - 1; lo <= hi;) {
-            const int mid = (lo + hi) >> 1;
-            if (nd.pops[mid].begin <= id) { pi = mid; lo = mid + 1; } else hi = mid - 1;
+    if (threadIdx.x < 32) {
+        uint32_t carry = 0;
+        for (int m0 = 1; m0 <= D; m0 += 32) {
+            int m = m0 + (int)lane;
+            uint32_t c = (m <= D) ? s_pre[m] : 0u;
+            uint32_t incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (uint32_t)o) incl += y;
+            }
+            if (m <= D) s_pre[m] = carry + incl;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
         }
-        if (pi >= 0 && id >= nd.pops[pi].end) pi = -1;
-        if (pi >= 0) {
-            const PopDev* pd = &nd.pops[pi];
-            PopParams p{pd, id - pd->begin, pd->end - pd->begin};
-            const bool f = forced ? ((forced[id >> 5] >> (id & 31)) & 1u) : false;
-            const int model = pd->model;
-            if (id < nd.N) {
-                float in_e, in_i;
-                if (nd.acc_mode == SZSNN_ACC_FIXED) {
-                    in_e = __ll2float_rn(nd.fx_e[id]) * (1.0f / 4294967296.0f);
-                    in_i = __ll2float_rn(nd.fx_i[id]) * (1.0f / 4294967296.0f);
-                    nd.fx_e[id] = 0;
-                    nd.fx_i[id] = 0;
-                } else {
-                    in_e = nd.in_e[id];
-                    in_i = nd.in_i[id];
-                    nd.in_e[id] = 0.0f;
-                    nd.in_i[id] = 0.0f;
+    }
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        nd.ring_cnt[t % R] = 0;
+        if (t >= 1) atomicAdd(&nd.stats[1], (unsigned long long)(s_pre[1]));
+    }
+    const uint32_t total = s_pre[D];
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int2* __restrict__ syn = nd.syn;
+    uint32_t ev = 0;
+    for (int64_t base = gw * IPW; base < (int64_t)total; base += nw * IPW) {
+        const int64_t item = base + lane;
+        unsigned long long a = 0, e = 0;
+        if (lane < (uint32_t)IPW && item < (int64_t)total) {
+            int lo = 1, hi = D;
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if ((int64_t)s_pre[mid] > item) hi = mid; else lo = mid + 1;
+            }
+            const int m = lo;
+            const uint32_t j = (uint32_t)(item - s_pre[m - 1]);
+            const int64_t s = __ldg(&nd.ring_ids[((t - m) % R) * nd.U + j]);
+            a = __ldg(&nd.row_ptr[s * D + (m - 1)]);
+            e = __ldg(&nd.row_ptr[s * D + m]);
+        }
+        const uint32_t len = (uint32_t)(e - a);
+        uint32_t incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += y;
+        }
+        const uint32_t excl = incl - len;
+        const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+        for (uint32_t k0 = 0; k0 < tot; k0 += 32 * UNR) {
+            int2 sw[UNR];
+            bool ok[UNR];
+#pragma unroll
+            for (int u = 0; u < UNR; ++u) {
+                const uint32_t k = k0 + 32u * u + lane;
+                ok[u] = k < tot;
+                int owner = 0;  // last lane whose segment starts at or before k
+#pragma unroll
+                for (int st = 16; st >= 1; st >>= 1) {
+                    const int cand = owner + st;
+                    const uint32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
+                    if (cand < 32 && ex <= k) owner = cand;
                 }
-                if (nd.dbg_in_e) { nd.dbg_in_e[id] = in_e; nd.dbg_in_i[id] = in_i; }
-                const float i_ext = current ? current[id] : 0.0f;
-                if (model == SZSNN_IF_CURR_EXP || model == SZSNN_IF_COND_EXP) {
-                    float v = nd.st0[id], g1 = nd.st1[id], g2 = nd.st2[id], fr = nd.st3[id];
-                    if (model == SZSNN_IF_CURR_EXP) spk = sz_if_curr_exp(p, v, g1, g2, fr, in_e, in_i, i_ext, f);
-                    else spk = sz_if_cond_exp(p, v, g1, g2, fr, in_e, in_i, i_ext, f);
-                    nd.st0[id] = v; nd.st1[id] = g1; nd.st2[id] = g2; nd.st3[id] = fr;
-                } else if (model == SZSNN_IZHIKEVICH) {
-                    float v = nd.st0[id], u = nd.st1[id];
-                    spk = sz_izhikevich(p, v, u, in_e, in_i, i_ext, f, (pd->flags & SZSNN_POP_IZH_HALF_STEPS) != 0);
-                    nd.st0[id] = v; nd.st1[id] = u;
-                }
-            } else {
-                if (model == SZSNN_POISSON) {
-                    spk = sz_poisson_fires(pd->seed, id, t, p(0)) || f;
-                } else if (model == SZSNN_CONST_RATE) {
-                    float last = nd.st0[id];
-                    spk = sz_const_rate(p, last, f);
-                    nd.st0[id] = last;
+                const unsigned long long oa = __shfl_sync(0xffffffffu, a, owner);
+                const uint32_t oex = __shfl_sync(0xffffffffu, excl, owner);
+                sw[u] = ok[u] ? __ldg(&syn[oa + (k - oex)]) : make_int2(0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < UNR; ++u) {
+                const float w = __int_as_float(sw[u].y);
+                if (ok[u] && w != 0.0f) {
+                    if ((unsigned long long)sw[u].x >= (unsigned long long)nd.N) {
+                        dev_error(nd.err, SZSNN_DEV_BAD_TARGET, (uint32_t)sw[u].x);
+                        continue;
+                    }
+                    ++ev;
+                    if (nd.acc_mode == SZSNN_ACC_FIXED) {
+                        long long qv = __float2ll_rn(w * 4294967296.0f);
+                        atomicAdd((unsigned long long*)(w >= 0.0f ? &nd.fx_e[sw[u].x] : &nd.fx_i[sw[u].x]),
+                                  (unsigned long long)qv);
+                    } else {
+                        atomicAdd(w >= 0.0f ? &nd.in_e[sw[u].x] : &nd.in_i[sw[u].x], w);
+                    }
                 }
             }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
+    if (lane == 0 && ev) atomicAdd(&s_ev, (unsigned long long)ev);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_ev) atomicAdd(&nd.stats[0], s_ev);
+}
+
+// last population with begin <= id, or -1 (ranges sorted and disjoint)
+__device__ __forceinline__ int find_pop(const PopDev* pops, int npops, int64_t id)
+{
+    int pi = -1;
+    for (int lo = 0, hi = npops - 1; lo <= hi;) {
+        const int mid = (lo + hi) >> 1;
+        if (pops[mid].begin <= id) { pi = mid; lo = mid + 1; } else hi = mid - 1;
+    }
+    return pi;
+}
+
+#define UPD_BLOCK_POPS 8
+
+// One thread per unit.  Thread 0 stages the populations overlapping the
+// block (and the step counter) in shared memory while every thread already
+// has its state loads in flight, so each thread's chain of dependent global
+// accesses is: state / input loads -> model arithmetic -> stores.
+__global__ void __launch_bounds__(1024) k_update(NetDev nd, int k_off, const uint32_t* __restrict__ forced,
+                                                const float* __restrict__ current, uint32_t* __restrict__ out_words)
+{
+    __shared__ PopDev s_pop[UPD_BLOCK_POPS];
+    __shared__ int s_np;  // populations staged, -1 when more overlap the block (global lookup)
+    __shared__ long long s_t;
+    const int64_t b0 = (int64_t)blockIdx.x * blockDim.x;
+    const int64_t id = b0 + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31;
+    // populations overlapping the block: the whole table when it is small, else
+    // the host-computed (first, count) of this block; one cooperative copy
+    int first = 0, np = nd.npops;
+    if (np > UPD_BLOCK_POPS) {
+        const int2 fc = nd.blk_pop[blockIdx.x];
+        first = fc.x;
+        np = fc.y > UPD_BLOCK_POPS ? -1 : fc.y;
+    }
+    if (np > 0) {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(nd.pops + first);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(s_pop);
+        for (int w = threadIdx.x; w < np * (int)(sizeof(PopDev) / 8); w += blockDim.x) dst[w] = src[w];
+    }
+    if (threadIdx.x == 0) { s_np = np; s_t = *nd.clock + k_off; }
+    float* __restrict__ st0 = nd.st0;
+    float* __restrict__ st1 = nd.st1;
+    float* __restrict__ st2 = nd.st2;
+    float* __restrict__ st3 = nd.st3;
+    const bool unit = id < nd.U, neuron = id < nd.N;
+    float v = 0.0f, g1 = 0.0f, g2 = 0.0f, fr = 0.0f, in_e = 0.0f, in_i = 0.0f, i_ext = 0.0f;
+    long long fxe = 0, fxi = 0;
+    if (unit) v = st0[id];
+    if (neuron) {
+        g1 = st1[id];
+        g2 = st2[id];
+        fr = st3[id];
+        if (nd.acc_mode == SZSNN_ACC_FIXED) { fxe = nd.fx_e[id]; fxi = nd.fx_i[id]; }
+        else { in_e = nd.in_e[id]; in_i = nd.in_i[id]; }
+        if (current) i_ext = current[id];
+    }
+    const bool f = (forced && unit) ? ((forced[id >> 5] >> (id & 31)) & 1u) : false;
+    __syncthreads();
+    const long long t = s_t;
+    const PopDev* pd = nullptr;
+    if (unit) {
+        const int np = s_np;
+        if (np >= 0) {
+            for (int i = 0; i < np; ++i)
+                if (id >= s_pop[i].begin && id < s_pop[i].end) { pd = &s_pop[i]; break; }
+        } else {
+            const int pi = find_pop(nd.pops, nd.npops, id);
+            if (pi >= 0 && id < nd.pops[pi].end) pd = &nd.pops[pi];
+        }
+    }
+    bool spk = false;
+    if (pd) {
+        const int model = pd->model;
+        if (neuron) {
+            if (nd.acc_mode == SZSNN_ACC_FIXED) {
+                in_e = __ll2float_rn(fxe) * (1.0f / 4294967296.0f);
+                in_i = __ll2float_rn(fxi) * (1.0f / 4294967296.0f);
+                nd.fx_e[id] = 0;
+                nd.fx_i[id] = 0;
+            } else {
+                nd.in_e[id] = 0.0f;
+                nd.in_i[id] = 0.0f;
+            }
+            if (nd.dbg_in_e) { nd.dbg_in_e[id] = in_e; nd.dbg_in_i[id] = in_i; }
+            if (pd->pn) spk = run_neuron(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, model, pd->flags,
+                                         v, g1, g2, fr, in_e, in_i, i_ext, f);
+            else spk = run_neuron(SharedParams{pd->p}, model, pd->flags, v, g1, g2, fr, in_e, in_i, i_ext, f);
+            st0[id] = v;
+            st1[id] = g1;
+            if (model != SZSNN_IZHIKEVICH) { st2[id] = g2; st3[id] = fr; }
+        } else if (model == SZSNN_POISSON) {
+            const float prob = pd->pn ? pd->pn[id - pd->begin] : pd->p[0];
+            spk = sz_poisson_fires(pd->seed, id, t, prob) || f;
+        } else if (model == SZSNN_CONST_RATE) {
+            if (pd->pn) spk = sz_const_rate(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, v, f);
+            else spk = sz_const_rate(SharedParams{pd->p}, v, f);
+            st0[id] = v;
         }
     }
     if (spk && nd.group) atomicAdd(&nd.group_spikes[nd.group[id]], 1ull);
@@ -392,13 +568,22 @@ NetDev make_dev(szsnn_net* n)
     d.clock = n->d_clock; d.stats = n->d_stats; d.err = n->ctx->d_err;
     d.dbg_in_e = nullptr; d.dbg_in_i = nullptr;
     d.group = n->d_group; d.group_spikes = n->d_group_spikes;
+    d.blk_pop = n->d_blk_pop;
     return d;
 }
 
 cudaError_t launch_propagate(szsnn_net* n, const NetDev& d, int k_off)
 {
-    int blocks = n->prop_blocks > 0 ? n->prop_blocks : num_sms(n->ctx) * 8;
+    int blocks = n->prop_blocks > 0 ? n->prop_blocks : num_sms(n->ctx) * 16;
     cudaStream_t st = n->ctx->stream;
+    if (n->prop_mode == 1) {
+        switch (n->prop_group) {
+        case 8: k_propagate_flat<8><<<blocks, 256, 0, st>>>(d, k_off); break;
+        case 16: k_propagate_flat<16><<<blocks, 256, 0, st>>>(d, k_off); break;
+        default: k_propagate_flat<32><<<blocks, 256, 0, st>>>(d, k_off); break;
+        }
+        return cudaGetLastError();
+    }
     switch (n->prop_group) {
     case 4: k_propagate<4><<<blocks, 256, 0, st>>>(d, k_off); break;
     case 8: k_propagate<8><<<blocks, 256, 0, st>>>(d, k_off); break;
@@ -406,6 +591,30 @@ cudaError_t launch_propagate(szsnn_net* n, const NetDev& d, int k_off)
     default: k_propagate<16><<<blocks, 256, 0, st>>>(d, k_off); break;
     }
     return cudaGetLastError();
+}
+
+// (first pop, count) overlapping each update block of `bs` threads
+cudaError_t fill_blk_pop(szsnn_net* n)
+{
+    if (n->npops <= UPD_BLOCK_POPS) return cudaSuccess;
+    const int bs = n->upd_block;
+    const int64_t nb = sz_div_up(n->U, bs);
+    std::vector<int2> t((size_t)nb);
+    int first = 0;
+    for (int64_t b = 0; b < nb; ++b) {
+        const int64_t b0 = b * bs, b1 = b0 + bs;
+        while (first < n->npops && n->pops[(size_t)first].end <= b0) ++first;
+        int c = 0;
+        for (int i = first; i < n->npops && n->pops[(size_t)i].begin < b1; ++i) ++c;
+        t[(size_t)b] = make_int2(first, c);
+    }
+    if (!n->d_blk_pop) {
+        cudaError_t e = cudaMalloc((void**)&n->d_blk_pop, (size_t)sz_div_up(n->U, 32) * sizeof(int2));
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = cudaMemcpyAsync(n->d_blk_pop, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, n->ctx->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(n->ctx->stream);
 }
 
 cudaError_t launch_update(szsnn_net* n, const NetDev& d, int k_off, const uint32_t* forced, const float* cur,
@@ -434,6 +643,7 @@ void free_net(szsnn_net* n)
     cudaFree(n->d_pn);
     cudaFree(n->d_group);
     cudaFree(n->d_group_spikes);
+    cudaFree(n->d_blk_pop);
     cudaFree(n->d_row_ptr);
     cudaFree(n->d_syn);
     for (int k = 0; k < 4; ++k) cudaFree(n->d_st[k]);
@@ -524,27 +734,39 @@ extern "C" int szsnn_net_create(szsnn_ctx* ctx, const szsnn_net_desc* d, szsnn_n
         std::vector<PopDev> hp((size_t)std::max(d->n_pops, 1));
         size_t pn_total = 0;
         for (int i = 0; i < d->n_pops; ++i)
-            if (d->pops[i].pn_host && d->pops[i].end > d->pops[i].begin) pn_total += (size_t)12 * (d->pops[i].end - d->pops[i].begin);
+            if (d->pops[i].pn_host && d->pops[i].end > d->pops[i].begin)
+                pn_total += (size_t)POP_SLOTS * (d->pops[i].end - d->pops[i].begin);
         if (pn_total) C(dalloc(&n->d_pn, pn_total));
         size_t off = 0;
+        std::vector<float> tmp;
         for (int i = 0; i < d->n_pops; ++i) {
             const szsnn_pop_desc& p = d->pops[i];
             PopDev& q = hp[(size_t)i];
             std::memset(&q, 0, sizeof(q));
             q.model = p.model; q.flags = p.flags; q.begin = p.begin; q.end = p.end;
-            std::memcpy(q.p, p.p, sizeof(q.p));
+            std::memcpy(q.p, p.p, sizeof(p.p));
+            const bool if_model = p.model == SZSNN_IF_CURR_EXP || p.model == SZSNN_IF_COND_EXP;
+            if (if_model) { q.p[12] = sz_decay(p.p[4]); q.p[13] = sz_decay(p.p[5]); }
             q.seed = p.seed;
             if (p.pn_host && p.end > p.begin) {
-                size_t cnt = (size_t)12 * (p.end - p.begin);
-                C(cudaMemcpyAsync(n->d_pn + off, p.pn_host, cnt * sizeof(float), cudaMemcpyHostToDevice, st));
+                const size_t cnt = (size_t)(p.end - p.begin);
+                tmp.assign((size_t)POP_SLOTS * cnt, 0.0f);
+                std::memcpy(tmp.data(), p.pn_host, 12 * cnt * sizeof(float));
+                if (if_model)
+                    for (size_t u = 0; u < cnt; ++u) {
+                        tmp[12 * cnt + u] = sz_decay(tmp[4 * cnt + u]);
+                        tmp[13 * cnt + u] = sz_decay(tmp[5 * cnt + u]);
+                    }
+                C(cudaMemcpy(n->d_pn + off, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice));
                 q.pn = n->d_pn + off;
-                off += cnt;
+                off += tmp.size();
             }
         }
         C(dalloc(&n->d_pops, hp.size()));
         C(cudaMemcpyAsync(n->d_pops, hp.data(), hp.size() * sizeof(PopDev), cudaMemcpyHostToDevice, st));
         C(cudaStreamSynchronize(st));
     }
+    C(fill_blk_pop(n));
     if (d->group_host) {
         for (int64_t i = 0; i < U; ++i)
             if (d->group_host[i] < 0 || d->group_host[i] >= d->n_groups) {
@@ -803,62 +1025,82 @@ extern "C" int szsnn_net_run_device(szsnn_net* n, int64_t steps, const uint32_t*
     return net_run_impl(n, steps, forced_dev, current_dev, raster_dev, false);
 }
 
-// Per-kernel device time: `steps` steps captured in one CUDA graph with an
-// event-record node after every kernel, so consecutive nodes run back to back
-// and each interval is one kernel's device time (no host launch gaps).
-extern "C" int szsnn_net_profile(szsnn_net* n, int64_t steps, double* prop_ms, double* upd_ms, double* total_ms)
+// Per-kernel device time.  The network's state, inputs, ring counters and
+// statistics are copied to scratch buffers; a CUDA graph then replays
+// `steps` propagate launches and `steps` update launches of the current step
+// (the clock does not advance, so every replay repeats the same work:
+// propagate reads the ring slots of steps t-1..t-D and only clears slot t,
+// update re-fills slot t of the scratch counters).  Events bracket each group
+// of launches on the launching stream; the real network is left untouched.
+extern "C" int szsnn_net_profile(szsnn_net* n, int64_t steps, double* prop_ms, double* upd_ms, double* events_per_launch)
 {
     if (!n || steps < 1 || steps > 100000) return SZSNN_ERR_ARG;
     cudaStream_t st = n->ctx->stream;
+    const size_t U = (size_t)n->U, N = (size_t)std::max<int64_t>(n->N, 1);
     NetDev d = make_dev(n);
-    std::vector<cudaEvent_t> ev((size_t)(2 * steps + 1));
-    for (auto& e : ev) NET_TRY(n, cudaEventCreate(&e));
+    float* sst[4] = {};
+    float *se = nullptr, *si = nullptr;
+    long long *sfe = nullptr, *sfi = nullptr;
+    uint32_t* scnt = nullptr;
+    unsigned long long* sstats = nullptr;
+    cudaEvent_t ev[3] = {};
     cudaGraph_t g = nullptr;
-    NET_TRY(n, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal);
-    for (int64_t k = 0; k < steps && e == cudaSuccess; ++k) {
-        e = launch_propagate(n, d, (int)k);
-        if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[(size_t)(2 * k + 1)], st, cudaEventRecordExternal);
-        if (e == cudaSuccess) e = launch_update(n, d, (int)k, nullptr, nullptr, nullptr);
-        if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[(size_t)(2 * k + 2)], st, cudaEventRecordExternal);
-    }
-    if (e == cudaSuccess) {
-        k_advance<<<1, 1, 0, st>>>(n->d_clock, (int)steps);
-        e = cudaGetLastError();
-    }
-    cudaError_t e2 = cudaStreamEndCapture(st, &g);
-    if (e != cudaSuccess || e2 != cudaSuccess) {
-        if (g) cudaGraphDestroy(g);
-        for (auto& x : ev) cudaEventDestroy(x);
-        return szsnn_set_error(n->ctx, SZSNN_ERR_CUDA,
-                               std::string("profile capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
-    }
     cudaGraphExec_t ex = nullptr;
-    e = cudaGraphInstantiate(&ex, g, 0);
-    cudaGraphDestroy(g);
-    NET_TRY(n, e);
-    NET_TRY(n, cudaGraphLaunch(ex, st));
-    NET_TRY(n, cudaStreamSynchronize(st));
-    cudaGraphExecDestroy(ex);
-    n->steps_done += steps;
-    n->kernel_launches += (uint64_t)2 * steps + 1;
-    n->graph_launches += 1;
-    double p = 0, u = 0;
-    for (int64_t k = 0; k < steps; ++k) {
-        float a = 0, b = 0;
-        cudaEventElapsedTime(&a, ev[(size_t)(2 * k)], ev[(size_t)(2 * k + 1)]);
-        cudaEventElapsedTime(&b, ev[(size_t)(2 * k + 1)], ev[(size_t)(2 * k + 2)]);
-        p += a;
-        u += b;
+    cudaError_t e = cudaSuccess;
+    auto fin = [&](cudaError_t err) {
+        if (ex) cudaGraphExecDestroy(ex);
+        if (g) cudaGraphDestroy(g);
+        for (auto& x : ev) if (x) cudaEventDestroy(x);
+        for (auto& x : sst) cudaFree(x);
+        cudaFree(se); cudaFree(si); cudaFree(sfe); cudaFree(sfi); cudaFree(scnt); cudaFree(sstats);
+        return err;
+    };
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
+        e = dalloc(&sst[k], U);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sst[k], n->d_st[k], U * 4, cudaMemcpyDeviceToDevice, st);
     }
-    float tot = 0;
-    cudaEventElapsedTime(&tot, ev[0], ev.back());
-    for (auto& x : ev) cudaEventDestroy(x);
-    n->t_prop_ms = p;
-    n->t_upd_ms = u;
-    if (prop_ms) *prop_ms = p;
-    if (upd_ms) *upd_ms = u;
-    if (total_ms) *total_ms = tot;
+    if (e == cudaSuccess) e = dalloc(&se, N);
+    if (e == cudaSuccess) e = dalloc(&si, N);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(se, n->d_in_e, N * 4, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(si, n->d_in_i, N * 4, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && n->acc_mode == SZSNN_ACC_FIXED) {
+        e = dalloc(&sfe, N);
+        if (e == cudaSuccess) e = dalloc(&sfi, N);
+        if (e == cudaSuccess) e = cudaMemsetAsync(sfe, 0, N * 8, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(sfi, 0, N * 8, st);
+    }
+    if (e == cudaSuccess) e = dalloc(&scnt, (size_t)n->R);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(scnt, n->d_ring_cnt, (size_t)n->R * 4, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = dalloc(&sstats, 4);
+    if (e == cudaSuccess) e = cudaMemsetAsync(sstats, 0, 32, st);
+    for (auto& x : ev) if (e == cudaSuccess) e = cudaEventCreate(&x);
+    if (e != cudaSuccess) return szsnn_set_error(n->ctx, SZSNN_ERR_CUDA, std::string("profile: ") + cudaGetErrorString(fin(e)));
+    d.st0 = sst[0]; d.st1 = sst[1]; d.st2 = sst[2]; d.st3 = sst[3];
+    d.in_e = se; d.in_i = si; d.fx_e = sfe; d.fx_i = sfi;
+    d.ring_cnt = scnt; d.stats = sstats; d.group = nullptr; d.group_spikes = nullptr;
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal);
+    for (int64_t k = 0; k < steps && e == cudaSuccess; ++k) e = launch_propagate(n, d, 0);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal);
+    for (int64_t k = 0; k < steps && e == cudaSuccess; ++k) e = launch_update(n, d, 0, nullptr, nullptr, nullptr);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal);
+    cudaError_t e2 = cudaStreamEndCapture(st, &g);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(ex, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    float a = 0, b = 0;
+    unsigned long long hs[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&a, ev[0], ev[1]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&b, ev[1], ev[2]);
+    if (e == cudaSuccess) e = cudaMemcpy(hs, sstats, sizeof(hs), cudaMemcpyDeviceToHost);
+    fin(cudaSuccess);
+    if (e != cudaSuccess) return szsnn_set_error(n->ctx, SZSNN_ERR_CUDA, std::string("profile: ") + cudaGetErrorString(e));
+    n->t_prop_ms = a;
+    n->t_upd_ms = b;
+    if (prop_ms) *prop_ms = a;
+    if (upd_ms) *upd_ms = b;
+    if (events_per_launch) *events_per_launch = (double)hs[0] / (double)steps;
     return SZSNN_OK;
 }
 
@@ -877,16 +1119,21 @@ extern "C" int szsnn_net_timing(szsnn_net* n, double* prop_ms, double* upd_ms, d
     return SZSNN_OK;
 }
 
-extern "C" int szsnn_net_set_tuning(szsnn_net* n, int group, int blocks, int upd_block)
+extern "C" int szsnn_net_set_tuning(szsnn_net* n, int mode, int group, int blocks, int upd_block)
 {
     if (!n) return SZSNN_ERR_ARG;
-    if (group != 0 && group != 4 && group != 8 && group != 16 && group != 32)
-        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "propagate group must be 4, 8, 16 or 32");
+    if (mode != 0 && mode != 1) return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "propagate mode must be 0 or 1");
+    if (mode == 0 && group != 0 && group != 4 && group != 8 && group != 16 && group != 32)
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "grouped propagate: lanes per bucket must be 4, 8, 16 or 32");
+    if (mode == 1 && group != 0 && group != 8 && group != 16 && group != 32)
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "flattened propagate: items per warp must be 8, 16 or 32");
     if (upd_block != 0 && (upd_block < 32 || upd_block > 1024 || upd_block % 32))
         return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "update block must be a multiple of 32 in 32..1024");
-    if (group) n->prop_group = group;
+    n->prop_mode = mode;
+    n->prop_group = group ? group : (mode == 1 ? 32 : 16);
     if (blocks >= 0) n->prop_blocks = blocks;
     if (upd_block) n->upd_block = upd_block;
+    NET_TRY(n, fill_blk_pop(n));
     for (auto& kv : n->graphs) cudaGraphExecDestroy(kv.second);
     n->graphs.clear();
     return SZSNN_OK;

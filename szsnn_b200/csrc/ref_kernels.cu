@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(1024) k_ref_update(RefUpdateArgs a)
         float* var = a.vars + (size_t)P * a.mps + n;
         if (MODEL == M_IF_CURR) {
             float v = var[0], ie = var[step], ii = var[2 * step], fired = var[3 * step];
-            spk = sz_if_curr_exp(p, v, ie, ii, fired, cur_e[n], cur_i[n], i_ext, forced);
+            spk = sz_if_curr_exp(p, v, ie, ii, fired, cur_e[n], cur_i[n], i_ext, forced, sz_decay(p(4)), sz_decay(p(5)));
             var[0] = v; var[step] = ie; var[2 * step] = ii; var[3 * step] = fired;
         } else if (MODEL == M_IZH) {
             float v = var[0], u = var[step];

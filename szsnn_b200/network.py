@@ -163,12 +163,15 @@ class Network:
                 "net_run_device")
 
     def profile(self, steps: int) -> tuple[float, float, float]:
-        p, u, t = C.c_double(), C.c_double(), C.c_double()
-        L.check(self.lib.szsnn_net_profile(self.h, steps, C.byref(p), C.byref(u), C.byref(t)), self.ctx.h, "profile")
-        return p.value, u.value, t.value
+        """(propagate ms, update ms) summed over `steps` replays of the current
+        step on scratch state, and the events one propagate launch delivers."""
+        p, u, ev = C.c_double(), C.c_double(), C.c_double()
+        L.check(self.lib.szsnn_net_profile(self.h, steps, C.byref(p), C.byref(u), C.byref(ev)), self.ctx.h,
+                "profile")
+        return p.value, u.value, ev.value
 
-    def set_tuning(self, group: int = 0, blocks: int = -1, update_block: int = 0) -> None:
-        L.check(self.lib.szsnn_net_set_tuning(self.h, group, blocks, update_block), self.ctx.h, "set_tuning")
+    def set_tuning(self, mode: int = 0, group: int = 0, blocks: int = -1, update_block: int = 0) -> None:
+        L.check(self.lib.szsnn_net_set_tuning(self.h, mode, group, blocks, update_block), self.ctx.h, "set_tuning")
 
     def stats(self) -> dict:
         s = L.NetStats()

@@ -335,3 +335,20 @@ def test_native_bad_target_sets_device_error(ctx_prod):
     assert ctx_prod.device_error() == (1, n + 100)
     ctx_prod.clear_device_error()
     ctx_prod.sync()
+
+
+@pytest.mark.parametrize("mode,group,blocks,ub", [(0, 4, 148, 128), (0, 32, 592, 256), (1, 8, 296, 512),
+                                                   (1, 16, 1184, 256), (1, 32, 2368, 1024)])
+def test_launch_shapes_are_bit_identical(ctx_prod, mode, group, blocks, ub):
+    """Every propagate variant / launch shape gives the oracle's fixed-point result."""
+    n, p, D = 20000, 2000, 64
+    blocks_, pops, st = cond_network(n, p, D=D, seed=8)
+    net = sz.Network(ctx_prod, n, p, D, pops, state=st, acc_mode=L.ACC_FIXED)
+    net.generate(blocks_, seed=4242)
+    net.set_tuning(mode, group, blocks, ub)
+    on = oracle.OracleNet(n, p, D, pops, oracle.generate(blocks_, 4242, n + p, D), state=st)
+    r_gpu = net.run(150)
+    r_orc, ev = on.run(150, acc_mode=oracle.ACC_FIXED)
+    assert np.array_equal(r_gpu, r_orc)
+    assert np.array_equal(net.get_state(0), on.state[0])
+    assert net.stats()["events"] == ev
