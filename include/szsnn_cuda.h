@@ -322,6 +322,43 @@ int szsnn_net_timing(szsnn_net* net, double* propagate_ms, double* update_ms, do
  * warp (8/16/32); propagate grid blocks (0 = 16 per SM); update block size */
 int szsnn_net_set_tuning(szsnn_net* net, int propagate_mode, int group, int propagate_blocks, int update_block);
 
+/* ----------------------------------------- allocation-free single step ---
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- hosts that own and partition all of it (a fixed-budget pool or
+ * arena, a framework's caching allocator) and forbid libraries from calling
+ * cudaMalloc, or real-time loops that cannot take cudaMalloc's implicit device
+ * synchronisation -- szsnn_step_static runs one propagate + update step of a
+ * network held entirely in caller-provided device buffers (one neuron
+ * population of a single model and parameter set, plus optional Poisson
+ * sources).  The step's scratch (input accumulators and a small header) is a
+ * file-scope static device array of fixed size inside the library, held by
+ * every GPU that loads it until the process exits: at most
+ * SZSNN_STATIC_MAX_NEURONS neurons, larger networks return SZSNN_ERR_LIMIT.
+ * The first call on a device looks up the array's device address (make it
+ * before any stream capture).  Every call shares the array and clears what
+ * must start at zero; calls that overlap on the GPU race on it and must be
+ * serialised by the caller.  The call is asynchronous on `stream`. */
+#define SZSNN_STATIC_MAX_NEURONS 262144
+typedef struct {
+    int64_t  n_neurons, n_sources;
+    int32_t  max_delay;
+    int64_t  step;              /* absolute step number of this call */
+    int32_t  model;             /* SZSNN_IF_CURR_EXP, SZSNN_IF_COND_EXP or SZSNN_IZHIKEVICH */
+    uint32_t flags;             /* SZSNN_POP_IZH_HALF_STEPS */
+    float    params[12];        /* one parameter set, slots as szsnn_pop_desc */
+    float    source_p;          /* spike probability per step of every Poisson source */
+    uint64_t seed;
+    const uint64_t* row_ptr;    /* device, (N+P)*D+1, delay-bucketed rows */
+    const int32_t*  syn;        /* device, (target, fp32 weight bits) pairs */
+    float*    state[4];         /* device, N+P each, slots as szsnn_pop_desc */
+    uint32_t* ring_cnt;         /* device, D+1, zero before the first step */
+    int32_t*  ring_ids;         /* device, (D+1)*(N+P) */
+    uint32_t* fired_words;      /* device out, (N+P+31)/32 spike words, or NULL */
+    uint32_t* error_word;       /* device out, 2 words (code, info), or NULL */
+    void*     stream;           /* cudaStream_t, NULL = legacy default stream */
+} szsnn_static_step;
+int szsnn_step_static(const szsnn_static_step* s, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1310,3 +1310,125 @@ extern "C" int szsnn_net_last_inputs(szsnn_net* n, float* in_exc, float* in_inh)
     NET_TRY(n, cudaStreamSynchronize(st));
     return SZSNN_OK;
 }
+
+// ---------------------------------------------------------------------------
+// szsnn_step_static: one step that allocates nothing.
+//
+// For callers that cannot call cudaMalloc: hosts that own and partition all
+// device memory themselves (a fixed-budget pool or arena, a framework's
+// caching allocator) and forbid libraries from allocating, and real-time
+// step loops that cannot afford cudaMalloc's implicit device synchronisation
+// and unbounded latency.  The caller passes every input and output buffer;
+// the step's scratch -- the per-step input accumulators plus a small header
+// (step counter, statistics, population table, error word) -- lives in the
+// file-scope array below, which every GPU that loads this library holds until
+// the process exits.
+//
+// Limits and sharing: at most SZSNN_STATIC_MAX_NEURONS neurons (larger
+// networks are rejected with SZSNN_ERR_LIMIT).  All calls on a device share
+// the one array and it keeps the last call's contents; each call clears the
+// parts that must start at zero before it launches.  Calls whose work
+// overlaps on the GPU (different streams, or threads launching at once)
+// race on the array and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+#define SZSNN_STATIC_HDR_BYTES 4096
+static __device__ __align__(256) unsigned char
+    g_static_scratch[SZSNN_STATIC_HDR_BYTES + 2 * sizeof(float) * SZSNN_STATIC_MAX_NEURONS];
+
+#include <mutex>
+
+namespace {
+std::mutex g_static_mu;
+void* g_static_addr[64] = {};  // device address of g_static_scratch per device
+int g_static_sms[64] = {};
+
+int static_fail(char* err, size_t len, int code, const std::string& m)
+{
+    if (err && len) {
+        std::strncpy(err, m.c_str(), len - 1);
+        err[len - 1] = 0;
+    }
+    return code;
+}
+}  // namespace
+
+extern "C" int szsnn_step_static(const szsnn_static_step* s, char* err, size_t err_len)
+{
+    if (!s) return static_fail(err, err_len, SZSNN_ERR_ARG, "szsnn_step_static: null argument");
+    const int64_t N = s->n_neurons, P = s->n_sources, U = N + P;
+    const int D = s->max_delay;
+    if (N < 1 || P < 0 || D < 1 || D > 1024 || s->step < 0)
+        return static_fail(err, err_len, SZSNN_ERR_ARG, "szsnn_step_static: bad sizes or step");
+    if (N > SZSNN_STATIC_MAX_NEURONS)
+        return static_fail(err, err_len, SZSNN_ERR_LIMIT,
+                           "szsnn_step_static: " + std::to_string(N) + " neurons exceed the static scratch maximum of " +
+                               std::to_string(SZSNN_STATIC_MAX_NEURONS));
+    if (U > 0x7fffffffLL)
+        return static_fail(err, err_len, SZSNN_ERR_LIMIT, "szsnn_step_static: more than 2^31-1 units");
+    if (s->model != SZSNN_IF_CURR_EXP && s->model != SZSNN_IF_COND_EXP && s->model != SZSNN_IZHIKEVICH)
+        return static_fail(err, err_len, SZSNN_ERR_ARG, "szsnn_step_static: model must be a neuron model");
+    if (!s->row_ptr || (!s->syn && U > 0) || !s->state[0] || !s->state[1] || !s->state[2] || !s->state[3] ||
+        !s->ring_cnt || !s->ring_ids)
+        return static_fail(err, err_len, SZSNN_ERR_ARG, "szsnn_step_static: null device buffer");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64)
+        return static_fail(err, err_len, SZSNN_ERR_CUDA, std::string("szsnn_step_static: cudaGetDevice: ") + cudaGetErrorString(e));
+    unsigned char* base = nullptr;
+    int sms = 148;
+    {
+        // once per device, with that device current: the device address of the
+        // static array (the host-side symbol is only a stand-in for it)
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        if (!g_static_addr[dev]) {
+            void* ptr = nullptr;
+            e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+            if (e != cudaSuccess || !ptr)
+                return static_fail(err, err_len, SZSNN_ERR_CUDA,
+                                   std::string("szsnn_step_static: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            int v = 148;
+            if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) v = 148;
+            g_static_sms[dev] = v;
+            g_static_addr[dev] = ptr;
+        }
+        base = (unsigned char*)g_static_addr[dev];
+        sms = g_static_sms[dev];
+    }
+    cudaStream_t st = (cudaStream_t)s->stream;
+    // header layout: [0] step counter, [64] statistics, [128] error word, [256] population table
+    PopDev hp[2];
+    std::memset(hp, 0, sizeof(hp));
+    hp[0].model = s->model; hp[0].flags = s->flags; hp[0].begin = 0; hp[0].end = N;
+    std::memcpy(hp[0].p, s->params, sizeof(s->params));
+    if (s->model != SZSNN_IZHIKEVICH) { hp[0].p[12] = sz_decay(s->params[4]); hp[0].p[13] = sz_decay(s->params[5]); }
+    hp[1].model = SZSNN_POISSON; hp[1].begin = N; hp[1].end = U; hp[1].p[0] = s->source_p; hp[1].seed = s->seed;
+    const long long clock = s->step;
+    float* acc = (float*)(base + SZSNN_STATIC_HDR_BYTES);
+    e = cudaMemcpyAsync(base + 256, hp, sizeof(hp), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base, &clock, sizeof(clock), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(base + 64, 0, 64 + 8, st);       // statistics and error word
+    if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, 2 * sizeof(float) * (size_t)N, st);  // input accumulators
+    if (e != cudaSuccess)
+        return static_fail(err, err_len, SZSNN_ERR_CUDA, std::string("szsnn_step_static: set-up copy: ") + cudaGetErrorString(e));
+    NetDev d{};
+    d.N = N; d.U = U; d.words = sz_div_up(U, 32); d.D = D; d.npops = P > 0 ? 2 : 1;
+    d.pops = (const PopDev*)(base + 256);
+    d.row_ptr = (const unsigned long long*)s->row_ptr;
+    d.syn = (const int2*)s->syn;
+    d.st0 = s->state[0]; d.st1 = s->state[1]; d.st2 = s->state[2]; d.st3 = s->state[3];
+    d.in_e = acc; d.in_i = acc + N;
+    d.acc_mode = SZSNN_ACC_FLOAT;
+    d.ring_cnt = s->ring_cnt; d.ring_ids = s->ring_ids;
+    d.clock = (const long long*)base;
+    d.stats = (unsigned long long*)(base + 64);
+    d.err = s->error_word ? s->error_word : (uint32_t*)(base + 128);
+    k_propagate<16><<<sms * 16, 256, 0, st>>>(d, 0);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        k_update<<<(unsigned)sz_div_up(U, 256), 256, 0, st>>>(d, 0, nullptr, nullptr, s->fired_words);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess)
+        return static_fail(err, err_len, SZSNN_ERR_CUDA, std::string("szsnn_step_static: launch: ") + cudaGetErrorString(e));
+    return SZSNN_OK;
+}
