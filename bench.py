@@ -40,6 +40,11 @@ UNIT = "syn-events/s"
 DT_MS = 0.1
 BYTES_PER_EVENT = 8      # int32 target + fp32 weight, delay implied by the bucket
 BYTES_PER_NEURON = 48    # 16 B state read + 16 B write + 8 B input read + 8 B clear
+# DRAM bytes (read + write) per launch from single ncu captures (cold L2):
+# k_update at 1.1M units, the benchmark's unit count; k_propagate at 300k
+# neurons x 1000 synapses (152,640 events per launch), scaled by events.
+NCU_UPDATE_TRAFFIC = 24_420_352
+NCU_PROPAGATE_TRAFFIC_PER_EVENT = 5_706_752 / 152_640
 
 
 def parse():
@@ -266,12 +271,14 @@ def main():
     upd_gbs = upd_bytes / (upd_ms / steps_p * 1e-3) / 1e9
     if prop_ms >= upd_ms:
         dom = {"kernel": "k_propagate", "achieved": prop_gbs, "bytes_per_launch": prop_bytes,
-               "us_per_launch": prop_ms / steps_p * 1e3}
+               "us_per_launch": prop_ms / steps_p * 1e3,
+               "traffic": int(NCU_PROPAGATE_TRAFFIC_PER_EVENT * ev_launch)}
     else:
         dom = {"kernel": "k_update", "achieved": upd_gbs, "bytes_per_launch": upd_bytes,
-               "us_per_launch": upd_ms / steps_p * 1e3}
+               "us_per_launch": upd_ms / steps_p * 1e3,
+               "traffic": NCU_UPDATE_TRAFFIC if n + p == 1_100_000 else None}
     roofline = {"bound": "hbm", "achieved": round(dom["achieved"], 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(dom["achieved"] / hbm, 4), "traffic": None, "kernel": dom["kernel"],
+                "frac": round(dom["achieved"] / hbm, 4), "traffic": dom["traffic"], "kernel": dom["kernel"],
                 "peak_source": peak_kind,
                 "us_per_launch": round(dom["us_per_launch"], 3),
                 "algorithmic_bytes_per_launch": int(dom["bytes_per_launch"]),

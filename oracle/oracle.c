@@ -50,10 +50,11 @@ static inline float orc_param(const orc_pop* p, int slot, int64_t id)
     return p->p[slot];
 }
 
-/* Poisson draw: spike iff u24(philox) < p  (no reference counterpart) */
-static inline int orc_poisson_fires(uint64_t seed, int64_t id, int64_t step, float p)
+/* Poisson draw: spike iff u24(philox) < p, counter = index within the
+ * population (no reference counterpart) */
+static inline int orc_poisson_fires(uint64_t seed, int64_t idx, int64_t step, float p)
 {
-    orc_u32x4 r = orc_philox((uint32_t)id, (uint32_t)step, (uint32_t)((uint64_t)step >> 32),
+    orc_u32x4 r = orc_philox((uint32_t)idx, (uint32_t)step, (uint32_t)((uint64_t)step >> 32),
                              ORC_STREAM_POISSON, (uint32_t)seed, (uint32_t)(seed >> 32));
     return orc_u24(r.v[0]) < p;
 }
@@ -71,7 +72,7 @@ void orc_gen_fixed_fanout(const orc_gen_block* b, uint64_t seed, int32_t D,
         memset(cnt, 0, sizeof(uint32_t) * (size_t)(D + 1));
         /* pass 1: delay histogram */
         for (int k = 0; k < F; ++k) {
-            orc_u32x4 x = orc_philox((uint32_t)s, (uint32_t)k, b->stream, ORC_STREAM_GEN, k0, k1);
+            orc_u32x4 x = orc_philox((uint32_t)r, (uint32_t)k, b->stream, ORC_STREAM_GEN, k0, k1);
             int m = b->d_lo + (int)orc_bounded(x.v[2], (uint32_t)(b->d_hi - b->d_lo + 1));
             cnt[m] += 1;
         }
@@ -84,7 +85,7 @@ void orc_gen_fixed_fanout(const orc_gen_block* b, uint64_t seed, int32_t D,
         }
         /* pass 2: stable placement by delay */
         for (int k = 0; k < F; ++k) {
-            orc_u32x4 x = orc_philox((uint32_t)s, (uint32_t)k, b->stream, ORC_STREAM_GEN, k0, k1);
+            orc_u32x4 x = orc_philox((uint32_t)r, (uint32_t)k, b->stream, ORC_STREAM_GEN, k0, k1);
             int64_t t;
             if (b->exclude_self && s >= b->tgt_begin && s < b->tgt_begin + b->tgt_count) {
                 t = b->tgt_begin + orc_bounded(x.v[0], (uint32_t)(b->tgt_count - 1));

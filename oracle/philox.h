@@ -3,15 +3,15 @@
  *
  * TEST INFRASTRUCTURE ONLY: this header belongs to the oracle (the CPU
  * restatement used to check the CUDA path).  The product keeps its own device
- * implementation in szsnn_b200/csrc/philox.cuh; both follow the published
+ * implementation in szsnn_b200/csrc/common.cuh; both follow the published
  * algorithm of Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
  * as 1, 2, 3", SC'11 (Philox-4x32, 10 rounds).  The two are compared
  * bit-for-bit by the parity tests.
  *
  * Stream conventions shared by oracle and device (the reference has no RNG on
  * its hot path; its only source model, Const_rate, is periodic):
- *   Poisson source draw : ctr = {id_lo, step_lo, step_hi, 0x504F4953}, key = seed
- *   network generator   : ctr = {src, k, block_stream, 0x53594E47}, key = seed
+ *   Poisson source draw : ctr = {index in population, step_lo, step_hi, 0x504F4953}, key = seed
+ *   network generator   : ctr = {row in block, k, block_stream, 0x53594E47}, key = seed
  *   uniform float       : (r >> 8) * 2^-24, exact in fp32, range [0, 1)
  *   bounded integer     : (uint32)(((uint64)r * range) >> 32)
  */

@@ -59,8 +59,10 @@ __device__ __forceinline__ void dev_error(uint32_t* err, uint32_t code, uint32_t
 
 // ---------------------------------------------------------------- Philox
 // Philox4x32-10 (Salmon et al., SC'11).  Counter / key conventions:
-//   Poisson draw  : ctr {id, step_lo, step_hi, 0x504F4953}, key = seed
-//   generator     : ctr {src, k, stream, 0x53594E47},       key = seed
+//   Poisson draw  : ctr {index in population, step_lo, step_hi, 0x504F4953}, key = seed
+//   generator     : ctr {row in block, k, stream, 0x53594E47},            key = seed
+// (population- and block-relative, so a network draws the same streams
+// wherever it sits in a batch)
 #define SZ_PHILOX_M0 0xD2511F53u
 #define SZ_PHILOX_M1 0xCD9E8D57u
 #define SZ_PHILOX_W0 0x9E3779B9u
@@ -96,9 +98,9 @@ __host__ __device__ __forceinline__ uint32_t sz_bounded(uint32_t r, uint32_t ran
     return (uint32_t)(((uint64_t)r * (uint64_t)range) >> 32);
 }
 
-__device__ __forceinline__ bool sz_poisson_fires(uint64_t seed, int64_t id, int64_t step, float p)
+__device__ __forceinline__ bool sz_poisson_fires(uint64_t seed, int64_t idx, int64_t step, float p)
 {
-    uint4 r = sz_philox((uint32_t)id, (uint32_t)step, (uint32_t)((uint64_t)step >> 32), SZ_STREAM_POISSON,
+    uint4 r = sz_philox((uint32_t)idx, (uint32_t)step, (uint32_t)((uint64_t)step >> 32), SZ_STREAM_POISSON,
                         (uint32_t)seed, (uint32_t)(seed >> 32));
     return sz_u24(r.x) < p;
 }

@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(1024) k_update(NetDev nd, int k_off, const uin
             if (model != SZSNN_IZHIKEVICH) { st2[id] = g2; st3[id] = fr; }
         } else if (model == SZSNN_POISSON) {
             const float prob = pd->pn ? pd->pn[id - pd->begin] : pd->p[0];
-            spk = sz_poisson_fires(pd->seed, id, t, prob) || f;
+            spk = sz_poisson_fires(pd->seed, id - pd->begin, t, prob) || f;
         } else if (model == SZSNN_CONST_RATE) {
             if (pd->pn) spk = sz_const_rate(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, v, f);
             else spk = sz_const_rate(SharedParams{pd->p}, v, f);
@@ -458,7 +458,7 @@ struct GenDraw { int64_t t; float w; int m; };
 
 __device__ __forceinline__ GenDraw gen_draw(const GenDev& g, int64_t s, int k)
 {
-    uint4 x = sz_philox((uint32_t)s, (uint32_t)k, g.stream, SZ_STREAM_GEN, g.k0, g.k1);
+    uint4 x = sz_philox((uint32_t)(s - g.src_begin), (uint32_t)k, g.stream, SZ_STREAM_GEN, g.k0, g.k1);
     GenDraw d;
     if (g.exclude_self && s >= g.tgt_begin && s < g.tgt_begin + g.tgt_count) {
         d.t = g.tgt_begin + sz_bounded(x.x, (uint32_t)(g.tgt_count - 1));
@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(256) k_generate(GenDev g, int D, unsigned long
         for (int j = lane; j < D; j += 32) h[j] = 0;
         __syncwarp();
         for (int k = lane; k < F; k += 32) {
-            uint4 x = sz_philox((uint32_t)s, (uint32_t)k, g.stream, SZ_STREAM_GEN, g.k0, g.k1);
+            uint4 x = sz_philox((uint32_t)r, (uint32_t)k, g.stream, SZ_STREAM_GEN, g.k0, g.k1);
             int m = g.d_lo + (int)sz_bounded(x.z, (uint32_t)(g.d_hi - g.d_lo + 1));
             atomicAdd(&h[m - 1], 1u);
         }
