@@ -322,6 +322,53 @@ int szsnn_net_timing(szsnn_net* net, double* propagate_ms, double* update_ms, do
  * warp (8/16/32); propagate grid blocks (0 = 16 per SM); update block size */
 int szsnn_net_set_tuning(szsnn_net* net, int propagate_mode, int group, int propagate_blocks, int update_block);
 
+/* ------------------------------------------ differentiable IF_curr_exp ---
+ * BPTT for a recurrent IF_curr_exp layer (no reference counterpart; the
+ * forward rule is IF_curr_exp_update_kernel.cl:230-287 with dt folded to 1
+ * and tau_refrac 0, the channel of a weight is its sign as in
+ * gather_kernel.cl:172-178).  Inputs x_t are integrated in their step,
+ * recurrent spikes one step later; y_t = alpha y_{t-1} + Wout^T s_t, outputs
+ * ymax = max_t y_t (with its first argmax) and vsum = sum_t v_t.  The
+ * backward is exact except dH/du, replaced by 1/(1 + beta|u - v_thresh|)^2
+ * (beta <= 0: 0), with forward spikes kept and u recomputed from checkpoints
+ * every `checkpoint_every` steps.  All pointers are device pointers owned by
+ * the caller (e.g. torch tensors); `workspace` holds
+ * szsnn_bptt_workspace_bytes bytes.  Calls are asynchronous on `stream`. */
+typedef struct {
+    int32_t B, N, M, K, T, checkpoint_every;        /* trials (<= 64), neurons, inputs, readouts (<= 64), steps */
+    float v_rest, cm, tau_m, tau_refrac, tau_syn_E, tau_syn_I, i_offset, v_reset, v_thresh;  /* step units */
+    float alpha;                                    /* readout leak factor */
+    float beta;                                     /* surrogate slope */
+    int64_t nnz;                                    /* recurrent synapses */
+    const float* w_in;                              /* [M][N] */
+    const int64_t* rec_row_ptr;                     /* [N+1] CSR of the recurrent weights, row = presynaptic */
+    const int32_t* rec_col;                         /* [nnz] postsynaptic neuron */
+    const float* rec_val;                           /* [nnz] */
+    const float* w_out;                             /* [N][K] */
+    const uint32_t* x_bits;                         /* [T][B][ceil(M/32)] input spike words */
+    const float* v0;                                /* [B][N] initial membrane */
+    uint32_t* spikes;                               /* [T][B][ceil(N/32)] out: spike words */
+    float* ckpt;                                    /* [ceil(T/ck)][3][B][N] out: (Ie, Ii, v) checkpoints */
+    float* ymax;                                    /* [B][K] out */
+    int32_t* tmax;                                  /* [B][K] out */
+    float* vsum;                                    /* [B][N] out */
+    float* u_trace;                                 /* [T][B][N] out: pre-reset membrane, or NULL */
+    const float* g_ymax;                            /* [B][K] dL/dymax (backward), or NULL */
+    const float* g_vsum;                            /* [B][N] dL/dvsum (backward), or NULL */
+    float* dw_in;                                   /* [M][N] out (backward) */
+    float* dw_rec;                                  /* [nnz] out (backward) */
+    float* dw_out;                                  /* [N][K] out (backward) */
+    const int32_t* plan_ptr;                        /* recurrent plan (szsnn_b200.pyszsnn.build_plan) or NULL: */
+    const int32_t* plan_loc;                        /*   entries grouped by (chunk of plan_chunk postsynaptic */
+    const int32_t* plan_perm;                       /*   neurons, presynaptic row); loc = target - chunk start, */
+    int32_t plan_chunk;                             /*   perm = synapse index; ptr [chunks][N+1] */
+    void* workspace;
+    void* stream;                                   /* cudaStream_t */
+} szsnn_bptt_desc;
+int szsnn_bptt_workspace_bytes(const szsnn_bptt_desc* d, uint64_t* bytes);
+int szsnn_bptt_forward(const szsnn_bptt_desc* d, char* err, size_t err_len);
+int szsnn_bptt_backward(const szsnn_bptt_desc* d, char* err, size_t err_len);
+
 /* ----------------------------------------- allocation-free single step ---
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory -- hosts that own and partition all of it (a fixed-budget pool or

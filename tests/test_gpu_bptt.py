@@ -1,0 +1,153 @@
+"""GPU: the pyszsnn autograd function and its hand-written adjoint.
+
+  * forward spikes / readout against the FP64 reference forward;
+  * gradients against the FP64 BPTT reference run on the GPU's own forward
+    trajectory (its spikes and pre-reset membrane): max |g_gpu - g_ref| <=
+    1e-4 * max |g_ref| per weight tensor.  Against an FP64 forward of the same
+    spike trains the gradients differ by up to ~1e-4 as well: the surrogate's
+    slope (up to 2*beta) turns the fp32 forward's membrane rounding (~4e-7)
+    into that much gradient change; the test bounds it at 5e-4;
+  * finite differences of the GPU forward in the subthreshold regime with the
+    surrogate off (beta = 0: the exact derivative);
+  * checkpointing: results independent of the checkpoint interval.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import bptt_ref as R
+from szsnn_b200 import pyszsnn as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(N=300, M=60, K=6, B=4, T=130, density=0.1, w_in_scale=0.6, w_rec_scale=1.0, beta=10.0, ck=50, seed=0,
+           plan=False):
+    dev = torch.device("cuda")
+    rp, col, val = P.random_recurrent(N, density, seed, dev)
+    val = val * w_rec_scale
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    w_in = (torch.randn((M, N), generator=g) * w_in_scale / np.sqrt(M)).to(dev)
+    w_out = (torch.randn((N, K), generator=g) / np.sqrt(N)).to(dev)
+    rates = torch.rand(M, generator=g) * 50.0
+    x = P.poisson_bits(T, B, rates.to(dev), 1.0, seed)
+    v0 = (torch.rand((B, N), generator=g) * 0.5).to(dev)
+    net = P.LIFCurrExpRNN(N, M, K, rp, col, alpha=0.95, beta=beta, checkpoint_every=ck, use_plan=plan)
+    return net, w_in, val, w_out, x, v0
+
+
+def _dense(net, val):
+    N = net.n_neurons
+    W = np.zeros((N, N), np.float64)
+    rp = net.rec_row_ptr.cpu().numpy()
+    col = net.rec_col.cpu().numpy()
+    v = val.detach().cpu().numpy().astype(np.float64)
+    for j in range(N):
+        W[j, col[rp[j]:rp[j + 1]]] = v[rp[j]:rp[j + 1]]
+    return W
+
+
+def test_forward_matches_fp64_reference():
+    net, w_in, val, w_out, x, v0 = _setup()
+    out = P.simulate(net, w_in, val, w_out, x, v0)
+    torch.cuda.synchronize()
+    S_gpu = P.unpack_bits(out["spikes"], net.n_neurons).cpu().numpy()
+    xs = P.unpack_bits(x, net.n_inputs).cpu().numpy()
+    p = dict(net.params, alpha=net.alpha)
+    fw = R.forward(p, w_in.cpu().numpy(), _dense(net, val), w_out.cpu().numpy(), xs, v0.cpu().numpy())
+    assert S_gpu.sum() > 500
+    agree = (S_gpu == fw["S"].astype(bool)).mean()
+    assert np.array_equal(S_gpu[:20], fw["S"][:20].astype(bool))
+    assert agree > 0.999
+    # readout of the GPU's own spikes equals the FP64 readout of those spikes
+    fw2 = R.forward(p, w_in.cpu().numpy(), _dense(net, val), w_out.cpu().numpy(), xs, v0.cpu().numpy(), spikes=S_gpu)
+    assert np.allclose(out["ymax"].cpu().numpy(), fw2["ymax"], rtol=1e-5, atol=1e-5)
+    assert np.allclose(out["vsum"].cpu().numpy(), fw2["vsum"], rtol=1e-4, atol=1e-3)
+
+
+@pytest.mark.parametrize("ck,plan,N", [(50, True, 300), (13, True, 300), (50, False, 300), (50, True, 1000)])
+def test_gradients_match_fp64_bptt(ck, plan, N):
+    """plan: fused chunked recurrent backward (N=1000 spans three chunks) or
+    the per-row SpMM + weight-gradient kernels."""
+    net, w_in, val, w_out, x, v0 = _setup(ck=ck, plan=plan, N=N, T=130 if N <= 300 else 80)
+    w_in.requires_grad_(True)
+    val.requires_grad_(True)
+    w_out.requires_grad_(True)
+    ymax, vsum = P.LIFCurrExpFunction.apply(w_in, val, w_out, x, v0, net)
+    g = torch.Generator(device="cpu").manual_seed(1)
+    gy = torch.randn(ymax.shape, generator=g).cuda()
+    gv = (torch.randn(vsum.shape, generator=g) * 1e-3).cuda()
+    (ymax * gy).sum().add_((vsum * gv).sum()).backward()
+    torch.cuda.synchronize()
+    out = P.simulate(net, w_in.detach(), val.detach(), w_out.detach(), x, v0, trace_u=True)
+    S = P.unpack_bits(out["spikes"], net.n_neurons).cpu().numpy()
+    xs = P.unpack_bits(x, net.n_inputs).cpu().numpy()
+    p = dict(net.params, alpha=net.alpha)
+    Wd = _dense(net, val)
+    fw = R.forward(p, w_in.detach().cpu().numpy(), Wd, w_out.detach().cpu().numpy(), xs, v0.cpu().numpy(), spikes=S)
+    assert np.array_equal(fw["tmax"], out["tmax"].cpu().numpy())
+    fw_gpu = dict(fw, U=out["u_trace"].cpu().numpy().astype(np.float64))
+    rp, col = net.rec_row_ptr.cpu().numpy(), net.rec_col.cpu().numpy()
+    rows = np.repeat(np.arange(net.n_neurons), np.diff(rp))
+    for traj, bound in ((fw_gpu, 1e-4), (fw, 5e-4)):
+        dWin, dWrec, dWout = R.backward(p, w_in.detach().cpu().numpy(), Wd, w_out.detach().cpu().numpy(), xs, traj,
+                                        gy.cpu().numpy(), gv.cpu().numpy(), beta=net.beta)
+        for got, ref in ((w_in.grad, dWin), (val.grad, dWrec[rows, col]), (w_out.grad, dWout)):
+            got = got.cpu().numpy().astype(np.float64)
+            err = np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-30)
+            assert err <= bound, (err, bound)
+            assert np.max(np.abs(ref)) > 0
+
+
+def test_finite_differences_subthreshold():
+    """Below threshold the layer is linear in w_in on each sign pattern of the
+    weights (the sign picks the exc / inh synaptic channel), so a central
+    difference along a sign-preserving direction (w -> w (1 + eps n), |eps n|
+    < 1) is exact up to rounding.  The fp32 forward limits that rounding, so
+    the check uses one directional derivative over all input weights (large
+    signal) and a loss summed in fp64."""
+    net, w_in, val, w_out, x, v0 = _setup(w_in_scale=0.02, w_rec_scale=0.02, beta=0.0)
+    c = torch.randn((x.shape[1], net.n_neurons), generator=torch.Generator().manual_seed(3)).cuda()
+
+    def loss(wi):
+        ymax, vsum = P.LIFCurrExpFunction.apply(wi, val, w_out, x, v0, net)
+        return (vsum.double() * c.double()).sum()
+
+    wi = w_in.clone().requires_grad_(True)
+    loss(wi).backward()
+    n = torch.randn(w_in.shape, generator=torch.Generator().manual_seed(5)).clamp(-3, 3).cuda()
+    d = w_in * n
+    eps = 0.2
+    for wp in (w_in + eps * d, w_in - eps * d):
+        out = P.simulate(net, wp, val, w_out, x, v0)
+        assert int(P.unpack_bits(out["spikes"], net.n_neurons).sum()) == 0
+    with torch.no_grad():
+        fd = (float(loss(w_in + eps * d)) - float(loss(w_in - eps * d))) / (2 * eps)
+    ad = float((wi.grad.double() * d.double()).sum())
+    assert abs(fd - ad) <= 1e-3 * abs(fd), (fd, ad)
+
+
+def test_plan_and_row_kernels_agree():
+    """Both recurrent backward paths give the same gradients up to fp32
+    summation order."""
+    grads = []
+    for plan in (True, False):
+        net, w_in, val, w_out, x, v0 = _setup(N=800, B=37, plan=plan, seed=11)
+        val.requires_grad_(True)
+        ymax, vsum = P.LIFCurrExpFunction.apply(w_in, val, w_out, x, v0, net)
+        ymax.sum().backward()
+        grads.append(val.grad.clone())
+    scale = float(grads[1].abs().max())
+    assert scale > 0
+    assert float((grads[0] - grads[1]).abs().max()) <= 1e-5 * scale
+
+
+def test_checkpoint_interval_does_not_change_gradients():
+    grads = []
+    for ck in (50, 1000):
+        net, w_in, val, w_out, x, v0 = _setup(ck=ck, seed=7)
+        w_in.requires_grad_(True)
+        ymax, vsum = P.LIFCurrExpFunction.apply(w_in, val, w_out, x, v0, net)
+        ymax.sum().backward()
+        grads.append(w_in.grad.clone())
+    assert torch.equal(grads[0], grads[1])

@@ -266,3 +266,36 @@ def test_oracle_generator_and_fixed_point(built):
         rasters.append(r)
     assert np.array_equal(rasters[0], rasters[1])
     assert rasters[0][:, : n // 32].any()
+
+
+def test_bptt_reference_matches_finite_differences():
+    """FP64 BPTT reference: adjoint == central finite differences where no spike
+    flips (subthreshold, surrogate off: beta = 0 gives the exact derivative)."""
+    from oracle import bptt_ref as R
+
+    rng = np.random.default_rng(0)
+    T, B, M, N, K = 40, 3, 20, 30, 5
+    p = dict(v_rest=0.0, cm=1.0, tau_m=20.0, tau_syn_E=5.0, tau_syn_I=10.0, i_offset=0.0, v_reset=0.0,
+             v_thresh=1.0, alpha=0.95)
+    x = (rng.random((T, B, M)) < 0.1).astype(np.float64)
+    W_in = rng.normal(0, 0.004, (M, N))
+    W_rec = rng.normal(0, 0.004, (N, N)) * (rng.random((N, N)) < 0.3)
+    W_out = rng.normal(0, 1, (N, K))
+    v0 = rng.uniform(-0.5, 0.5, (B, N))
+    c = rng.normal(size=(B, N))
+
+    def loss(Wi):
+        fw = R.forward(p, Wi, W_rec, W_out, x, v0)
+        assert fw["S"].sum() == 0
+        return float((c * fw["vsum"]).sum()), fw
+
+    _, fw = loss(W_in)
+    dWin, _, _ = R.backward(p, W_in, W_rec, W_out, x, fw, None, c, beta=0.0)
+    eps = 1e-6
+    for _ in range(20):
+        j, i = rng.integers(M), rng.integers(N)
+        Wp, Wm = W_in.copy(), W_in.copy()
+        Wp[j, i] += eps
+        Wm[j, i] -= eps
+        fd = (loss(Wp)[0] - loss(Wm)[0]) / (2 * eps)
+        assert abs(fd - dWin[j, i]) <= 1e-7 * max(abs(fd), 1e-3)
