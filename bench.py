@@ -62,6 +62,11 @@ def parse():
     ap.add_argument("--cpu-neurons", type=int, default=50_000)
     ap.add_argument("--cpu-steps", type=int, default=300)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the batched-sweep and BPTT measurements")
+    ap.add_argument("--batch-nets", type=int, default=512)
+    ap.add_argument("--batch-steps", type=int, default=1000)
+    ap.add_argument("--bptt-scale", type=float, default=1.0)
+    ap.add_argument("--bptt-steps", type=int, default=500)
     return ap.parse_args()
 
 
@@ -164,6 +169,88 @@ def cpu_baseline(args, n_steps_warm=100):
                       f"{ev} events in {dt:.2f} s"}
 
 
+def bench_batched(ctx, args):
+    """Batched sweep: the nets/s of one block-diagonal run of `batch_nets`
+    uneven networks (N log-uniform 200..20,000, fan-out 100, delays U{1..20},
+    weight scale 0.5..2.0, Poisson 5..20 Hz, IF_curr_exp / Izhikevich
+    alternating, 100-step graphs, autotuned launch shape) against the plain
+    path looped over the same nets; device time on both sides."""
+    from szsnn_b200 import batch as B
+
+    specs = B.sweep_specs(args.batch_nets, seed=0)
+    r = B.compare_batched_looped(ctx, specs, steps=args.batch_steps, graph_chunk=100, tune=True)
+    same = bool(np.array_equal(r["spikes_batched"], r["spikes_looped"]))
+    return {"metric": "nets/s (batched sweep)", "nets": r["nets"], "steps": r["steps"],
+            "batched_nets_per_s": r["batched_nets_per_s"], "looped_nets_per_s": r["looped_nets_per_s"],
+            "speedup": r["speedup"], "batched_s": r["batched_s"], "looped_s": r["looped_s"],
+            "wall_batched_s": r["wall_batched_s"], "wall_looped_s": r["wall_looped_s"],
+            "neurons": r["neurons"], "synapses": r["synapses"],
+            "syn_events_per_s_batched": r["events_batched"] / r["batched_s"],
+            "spike_counts_equal_looped": same, "accumulation": "float",
+            "workload": f"{r['nets']} nets, N log-uniform 200..20000, fan-out 100, delays U{{1..20}} steps, "
+                        f"w scale 0.5..2.0, Poisson 5..20 Hz, dt 1 ms, {r['steps']} steps"}
+
+
+def bench_bptt(args):
+    """Differentiable IF_curr_exp RNN: one forward (simulate) against one
+    forward + cross-entropy + backward through the autograd function, batch 64
+    trials, 700 Poisson inputs (U(0,50) Hz), dense 700 x 10,000 input weights
+    |N(0,1)| * scale / sqrt(700), 10,000 neurons with 10 % random recurrent
+    weights N(0, 1/sqrt(fan-in)), 20 readouts, dt 1 ms, 500 steps, surrogate
+    slope 10, checkpoints every 50 steps.  CUDA events on torch's stream (the
+    stream the library launches on)."""
+    import torch
+    from szsnn_b200 import pyszsnn as P
+
+    dev = torch.device("cuda")
+    N, M, K, Bt, T = 10000, 700, 20, 64, args.bptt_steps
+    rp, col, val = P.random_recurrent(N, 0.1, 0, dev)
+    g = torch.Generator().manual_seed(0)
+    w_in = (torch.randn((M, N), generator=g).abs() * args.bptt_scale / np.sqrt(M)).to(dev)
+    w_out = (torch.randn((N, K), generator=g) / np.sqrt(N)).to(dev)
+    rates = (torch.rand(M, generator=g) * 50).to(dev)
+    x = P.poisson_bits(T, Bt, rates, 1.0, 0)
+    v0 = torch.zeros((Bt, N), device=dev)
+    labels = torch.randint(0, K, (Bt,), generator=g).to(dev)
+    net = P.LIFCurrExpRNN(N, M, K, rp, col, beta=10.0, checkpoint_every=50)
+    for t in (w_in, val, w_out):
+        t.requires_grad_(True)
+
+    def fwd():
+        return P.simulate(net, w_in.detach(), val.detach(), w_out.detach(), x, v0)
+
+    def fwdbwd():
+        for t in (w_in, val, w_out):
+            t.grad = None
+        ymax, _ = P.LIFCurrExpFunction.apply(w_in, val, w_out, x, v0, net)
+        loss = torch.nn.functional.cross_entropy(ymax, labels)
+        loss.backward()
+        return loss
+
+    for _ in range(2):
+        fwd()
+        fwdbwd()
+    torch.cuda.synchronize()
+    reps = 3
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record()
+    for _ in range(reps):
+        out = fwd()
+    e[1].record()
+    for _ in range(reps):
+        loss = fwdbwd()
+    e[2].record()
+    torch.cuda.synchronize()
+    f_ms = e[0].elapsed_time(e[1]) / reps
+    fb_ms = e[1].elapsed_time(e[2]) / reps
+    rate = float(P.unpack_bits(out["spikes"], N).float().mean()) * 1e3
+    return {"metric": "BPTT forward+backward cost / forward cost", "fwd_ms": f_ms, "fwd_bwd_ms": fb_ms,
+            "ratio": fb_ms / f_ms, "rate_hz": rate, "loss": float(loss.detach()), "trials": Bt, "steps": T,
+            "neurons": N, "inputs": M, "readouts": K, "synapses": int(col.numel()), "w_in_scale": args.bptt_scale,
+            "workload": "IF_curr_exp RNN 10,000 neurons (10 % recurrent), 700 Poisson inputs, 20 readouts, "
+                        "batch 64, 500 steps, fast-sigmoid slope 10, checkpoints every 50 steps"}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -176,6 +263,22 @@ def run_reference(args, rank):
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def reduce_replicas(dist, t, units):
+    """Replicas only: (max over ranks of the timed duration, sum over ranks of
+    the units processed).  Every rank calls it in the same order; `dist` is
+    torch.distributed (NCCL on GPUs, gloo in the CPU tests) or None."""
+    if dist is None:
+        return float(t), float(units)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    x = torch.tensor([float(t), float(units)], dtype=torch.float64, device=dev)
+    m = x[:1].clone()
+    dist.all_reduce(m, op=dist.ReduceOp.MAX)
+    u = x[1:].clone()
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(m.item()), float(u.item())
 
 
 def main():
@@ -203,13 +306,6 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    def allreduce(x, op):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=op)
-        return float(t.item())
 
     ctx = sz.Context(local_rank)
     n, p, D, blocks, pops = cond_config(args.neurons, args.fanout)
@@ -241,8 +337,7 @@ def main():
     ms_timed = tm.value if tm.value > 0 else t_wall * 1e3
     events = s1["events"] - s0["events"]
     spikes = s1["spikes"] - s0["spikes"]
-    ms_max = allreduce(ms_timed, dist.ReduceOp.MAX if dist else None)
-    ev_tot = allreduce(float(events), dist.ReduceOp.SUM if dist else None)
+    ms_max, ev_tot = reduce_replicas(dist, ms_timed, events)
     value = ev_tot / (ms_max / 1e3)
 
     # end to end through the public API: host input words in, host raster out, every step
@@ -256,8 +351,7 @@ def main():
     t_e2e = time.perf_counter() - t_e2e
     s3 = net.stats()
     e2e_events = s3["events"] - s2["events"]
-    e2e_max = allreduce(t_e2e, dist.ReduceOp.MAX if dist else None)
-    e2e_tot = allreduce(float(e2e_events), dist.ReduceOp.SUM if dist else None)
+    e2e_max, e2e_tot = reduce_replicas(dist, t_e2e, e2e_events)
     del raster, forced
 
     # per-kernel device time: replays of the current step on scratch state,
@@ -293,6 +387,19 @@ def main():
         except Exception as e:  # the baseline is reported, not required
             cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
 
+    n_syn, words = net.n_synapses, net.words
+    net.close()  # frees the 8 GB synapse table before the secondary workloads
+    batched = bptt = None
+    if rank == 0 and world == 1 and not args.no_secondary:
+        try:
+            batched = bench_batched(ctx, args)
+        except Exception as e:  # reported beside the headline, not required for it
+            batched = {"error": f"{type(e).__name__}: {e}"}
+        try:
+            bptt = bench_bptt(args)
+        except Exception as e:
+            bptt = {"error": f"{type(e).__name__}: {e}"}
+
     if rank == 0:
         steps = args.steps
         line = {
@@ -301,7 +408,7 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "IF_cond_exp 1M neurons x 1000 synapses (1e9), 100k Poisson x 100, "
                                    "delays U{1..64} steps, dt 0.1 ms",
-                       "neurons": n, "sources": p, "synapses": net.n_synapses, "max_delay": D,
+                       "neurons": n, "sources": p, "synapses": n_syn, "max_delay": D,
                        "accumulation": args.acc, "graph_chunk": 100,
                        "l2": "inputs larger than L2 (8 GB synapse table); neuron state L2-resident across steps",
                        "parallelism": f"replicas x{world}"},
@@ -312,13 +419,14 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cb,
             "e2e": {"value": e2e_tot / e2e_max, "unit": UNIT, "steps": e2e_steps,
-                    "h2d_bytes_per_step": int(net.words * 4), "d2h_bytes_per_step": int(net.words * 4),
+                    "h2d_bytes_per_step": int(words * 4), "d2h_bytes_per_step": int(words * 4),
                     "api": "szsnn_net_run (host forced-spike words in, host raster out)"},
             "gpu_launches": int(2 * steps + (steps + 99) // 100),
             "clocks": clk.summary(),
+            "batched": batched,
+            "bptt": bptt,
         }
         print(json.dumps(line), flush=True)
-    net.close()
     ctx.close()
     if dist is not None:
         dist.destroy_process_group()

@@ -162,6 +162,12 @@ class Network:
         L.check(self.lib.szsnn_net_run_device(self.h, steps, forced_ptr, current_ptr, raster_ptr), self.ctx.h,
                 "net_run_device")
 
+    def device_ms(self) -> float:
+        """Device time (CUDA events on the net's stream) of the last run / run_device."""
+        t = C.c_double()
+        L.check(L.lib().szsnn_net_timing(self.h, None, None, C.byref(t)), self.ctx.h, "net timing")
+        return float(t.value)
+
     def profile(self, steps: int) -> tuple[float, float, float]:
         """(propagate ms, update ms) summed over `steps` replays of the current
         step on scratch state, and the events one propagate launch delivers."""
