@@ -45,6 +45,7 @@ BYTES_PER_NEURON = 48    # 16 B state read + 16 B write + 8 B input read + 8 B c
 # neurons x 1000 synapses (152,640 events per launch), scaled by events.
 NCU_UPDATE_TRAFFIC = 24_420_352
 NCU_PROPAGATE_TRAFFIC_PER_EVENT = 5_706_752 / 152_640
+NCU_STEP_TRAFFIC = None  # k_step at 1.1M units: not captured yet
 
 
 def parse():
@@ -57,6 +58,11 @@ def parse():
     ap.add_argument("--fanout", type=int, default=1000)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--acc", default="float", choices=["float", "fixed"])
+    ap.add_argument("--classic", dest="overlap", action="store_false",
+                    help="propagate-then-update order (two launches per step) instead of the overlapped one")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="keep the default launch shape instead of autotuning after the warm-up")
+    ap.add_argument("--tune-after", type=int, default=3000, help="steps simulated before the tuner's replays")
     ap.add_argument("--e2e-steps", type=int, default=1000)
     ap.add_argument("--profile-steps", type=int, default=200)
     ap.add_argument("--cpu-neurons", type=int, default=50_000)
@@ -147,6 +153,17 @@ def peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def net_overlap(net) -> bool:
+    """The step order the network runs in (set by --classic or by the tuner)."""
+    return bool(net.overlap)
+
+
+def pinned_words(steps, words):
+    """uint32 [steps, words] in page-locked host memory (torch's pinned allocator)."""
+    import torch
+    return torch.empty((steps, words), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
 
 
 def cpu_baseline(args, n_steps_warm=100):
@@ -313,11 +330,24 @@ def main():
     net = sz.Network(ctx, n, p, D, pops, state=init_state(n, p, args.seed + rank), acc_mode=acc, graph_chunk=100)
     t0 = time.perf_counter()
     net.generate(blocks, seed=args.seed + 1000 * rank)
+    net.set_overlap(args.overlap)
     gen_s = time.perf_counter() - t0
 
-    # warm-up (graph instantiation, initial transient)
+    # warm-up (graph instantiation, initial transient), then the launch shape
+    # chosen by the autotuner on replays of a warmed-up step (scratch state)
     net.run_device(args.warmup)
     ctx.sync()
+    tuning = None
+    if args.tune:  # past the start-up transient (v(0) ~ U(-60,-50) fires a first volley)
+        from szsnn_b200.autotune import tune
+        net.run_device(max(0, args.tune_after - args.warmup))
+        ctx.sync()
+        ch = tune(net, replays=50, use_cache=False)
+        tuning = {k: ch[k] for k in ("overlap", "mode", "group", "blocks", "update_block", "step_us",
+                                     "classic_step_us")}
+        net.run_device(args.warmup)  # graphs of the chosen shape
+        ctx.sync()
+    overlap = net_overlap(net)
     s0 = net.stats()
     barrier()
     ctx.sync()
@@ -340,13 +370,15 @@ def main():
     ms_max, ev_tot = reduce_replicas(dist, ms_timed, events)
     value = ev_tot / (ms_max / 1e3)
 
-    # end to end through the public API: host input words in, host raster out, every step
+    # end to end through the public API: host input words in, host raster out,
+    # every step, both in page-locked host memory (DMA overlapped with compute)
     e2e_steps = min(args.e2e_steps, args.steps)
-    forced = np.zeros((e2e_steps, net.words), np.uint32)
+    forced, raster = pinned_words(e2e_steps, net.words), pinned_words(e2e_steps, net.words)
+    forced[:] = 0
     s2 = net.stats()
     barrier()
     t_e2e = time.perf_counter()
-    raster = net.run(e2e_steps, forced_words=forced, raster=True)
+    net.run(e2e_steps, forced_words=forced, out=raster)
     ctx.sync()
     t_e2e = time.perf_counter() - t_e2e
     s3 = net.stats()
@@ -356,29 +388,41 @@ def main():
 
     # per-kernel device time: replays of the current step on scratch state,
     # CUDA events on the launching stream around each group of launches
-    prop_ms, upd_ms, ev_launch = net.profile(args.profile_steps)
+    prof = net.profile_step(args.profile_steps)
     steps_p = args.profile_steps
+    ev_launch = prof["events_per_launch"]
+    hbm, peak_kind = peaks()
+    prop_us = prof["propagate_ms"] / steps_p * 1e3
+    upd_us = prof["update_ms"] / steps_p * 1e3
+    step_us = prof["step_ms"] / steps_p * 1e3
     prop_bytes = ev_launch * BYTES_PER_EVENT
     upd_bytes = n * BYTES_PER_NEURON
-    hbm, peak_kind = peaks()
-    prop_gbs = prop_bytes / (prop_ms / steps_p * 1e-3) / 1e9
-    upd_gbs = upd_bytes / (upd_ms / steps_p * 1e-3) / 1e9
-    if prop_ms >= upd_ms:
-        dom = {"kernel": "k_propagate", "achieved": prop_gbs, "bytes_per_launch": prop_bytes,
-               "us_per_launch": prop_ms / steps_p * 1e3,
+    ev_step = events / args.steps
+    if overlap:
+        # one fused launch per step (k_step): the update of every unit, the
+        # delay-1 buckets of its spikes and the delay >= 2 delivery of the next step
+        step_bytes = upd_bytes + ev_step * BYTES_PER_EVENT
+        dom = {"kernel": "k_step", "achieved": step_bytes / (step_us * 1e-6) / 1e9, "bytes_per_launch": step_bytes,
+               "us_per_launch": step_us, "traffic": NCU_STEP_TRAFFIC if n + p == 1_100_000 else None}
+    elif prop_us >= upd_us:
+        dom = {"kernel": "k_propagate", "achieved": prop_bytes / (prop_us * 1e-6) / 1e9,
+               "bytes_per_launch": prop_bytes, "us_per_launch": prop_us,
                "traffic": int(NCU_PROPAGATE_TRAFFIC_PER_EVENT * ev_launch)}
     else:
-        dom = {"kernel": "k_update", "achieved": upd_gbs, "bytes_per_launch": upd_bytes,
-               "us_per_launch": upd_ms / steps_p * 1e3,
-               "traffic": NCU_UPDATE_TRAFFIC if n + p == 1_100_000 else None}
+        dom = {"kernel": "k_update", "achieved": upd_bytes / (upd_us * 1e-6) / 1e9, "bytes_per_launch": upd_bytes,
+               "us_per_launch": upd_us, "traffic": NCU_UPDATE_TRAFFIC if n + p == 1_100_000 else None}
     roofline = {"bound": "hbm", "achieved": round(dom["achieved"], 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(dom["achieved"] / hbm, 4), "traffic": dom["traffic"], "kernel": dom["kernel"],
                 "peak_source": peak_kind,
                 "us_per_launch": round(dom["us_per_launch"], 3),
                 "algorithmic_bytes_per_launch": int(dom["bytes_per_launch"]),
-                "propagate": {"us_per_launch": round(prop_ms / steps_p * 1e3, 3), "gbs": round(prop_gbs, 1),
-                              "events_per_launch": ev_launch},
-                "update": {"us_per_launch": round(upd_ms / steps_p * 1e3, 3), "gbs": round(upd_gbs, 1)}}
+                "step": {"us": round(step_us, 3), "order": "overlapped" if overlap else "classic"},
+                "delivery_alone": {"us_per_launch": round(prop_us, 3),
+                                   "gbs": round(prop_bytes / (prop_us * 1e-6) / 1e9, 1),
+                                   "events_per_launch": ev_launch,
+                                   "delays": "2..64" if overlap else "1..64"},
+                "update_alone": {"us_per_launch": round(upd_us, 3),
+                                 "gbs": round(upd_bytes / (upd_us * 1e-6) / 1e9, 1)}}
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -410,6 +454,7 @@ def main():
                                    "delays U{1..64} steps, dt 0.1 ms",
                        "neurons": n, "sources": p, "synapses": n_syn, "max_delay": D,
                        "accumulation": args.acc, "graph_chunk": 100,
+                       "step_order": "overlapped" if overlap else "classic", "tuning": tuning,
                        "l2": "inputs larger than L2 (8 GB synapse table); neuron state L2-resident across steps",
                        "parallelism": f"replicas x{world}"},
             "neuron_updates_per_s": (n + p) * steps * world / (ms_max / 1e3),
@@ -420,8 +465,8 @@ def main():
             "cpu_baseline": cb,
             "e2e": {"value": e2e_tot / e2e_max, "unit": UNIT, "steps": e2e_steps,
                     "h2d_bytes_per_step": int(words * 4), "d2h_bytes_per_step": int(words * 4),
-                    "api": "szsnn_net_run (host forced-spike words in, host raster out)"},
-            "gpu_launches": int(2 * steps + (steps + 99) // 100),
+                    "api": "szsnn_net_run (forced-spike words in, raster out, page-locked host arrays)"},
+            "gpu_launches": int((1 if overlap else 2) * steps + (steps + 99) // 100),
             "clocks": clk.summary(),
             "batched": batched,
             "bptt": bptt,

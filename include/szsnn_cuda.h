@@ -314,6 +314,11 @@ int szsnn_net_last_inputs(szsnn_net* net, float* in_exc, float* in_inh);
  * synaptic events one propagate launch delivers */
 int szsnn_net_profile(szsnn_net* net, int64_t steps, double* propagate_ms, double* update_ms,
                       double* events_per_launch);
+/* As szsnn_net_profile, plus the device time of `steps` replays of the whole
+ * step (overlapped order: the fused k_step launch; classic: propagate +
+ * update), the time every simulated step costs. */
+int szsnn_net_profile_step(szsnn_net* net, int64_t steps, double* propagate_ms, double* update_ms, double* step_ms,
+                           double* events_per_launch);
 /* total_ms: device time (CUDA events on the stream) of the last szsnn_net_run /
  * szsnn_net_run_device; propagate/update: the last szsnn_net_profile */
 int szsnn_net_timing(szsnn_net* net, double* propagate_ms, double* update_ms, double* total_ms);
@@ -321,6 +326,14 @@ int szsnn_net_timing(szsnn_net* net, double* propagate_ms, double* update_ms, do
  * segment (4/8/16/32), mode 1 = warp-flattened walk over `group` items per
  * warp (8/16/32); propagate grid blocks (0 = 16 per SM); update block size */
 int szsnn_net_set_tuning(szsnn_net* net, int propagate_mode, int group, int propagate_blocks, int update_block);
+/* Step order.  1 (default): overlapped -- input buffers double-buffered by
+ * step parity, delivery of delays >= 2 into step t+1 runs on a second stream
+ * while update(t) runs, and update(t) delivers the delay-1 bucket of its own
+ * spikes.  0: classic -- propagate(t) delivers delays 1..D, then update(t)
+ * (the reference's order, Simulation.ipp:471-496).  Results are identical in
+ * fixed-point accumulation; switching mid-run rebuilds the next step's
+ * inputs from the spike ring. */
+int szsnn_net_set_overlap(szsnn_net* net, int overlap);
 
 /* ------------------------------------------ differentiable IF_curr_exp ---
  * BPTT for a recurrent IF_curr_exp layer (no reference counterpart; the

@@ -126,8 +126,10 @@ SIGNATURES = {
     "szsnn_net_check_finite": (_I, [_P, C.POINTER(C.c_int)]),
     "szsnn_net_last_inputs": (_I, [_P, _P, _P]),
     "szsnn_net_profile": (_I, [_P, _I64, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
+    "szsnn_net_profile_step": (_I, [_P, _I64, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
     "szsnn_net_timing": (_I, [_P, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
     "szsnn_net_set_tuning": (_I, [_P, _I, _I, _I, _I]),
+    "szsnn_net_set_overlap": (_I, [_P, C.c_int]),
     "szsnn_step_static": (_I, [_P, C.c_char_p, C.c_size_t]),
     "szsnn_bptt_workspace_bytes": (_I, [_P, C.POINTER(C.c_uint64)]),
     "szsnn_bptt_forward": (_I, [_P, C.c_char_p, C.c_size_t]),

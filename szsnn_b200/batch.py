@@ -129,7 +129,9 @@ def layout(specs: list[NetSpec]):
 
 
 class Batch:
-    """All nets of `specs` as one device network."""
+    """All nets of `specs` as one device network.  tune=True tunes at
+    construction (step 0); tuning after a warm-up (autotune.tune on .net) sees
+    the network's working event rate."""
 
     def __init__(self, ctx, specs: list[NetSpec], acc_mode: int = L.ACC_FLOAT, graph_chunk: int = 100,
                  gen_seed: int = 12345, tune: bool = False):
@@ -164,16 +166,23 @@ def single_network(ctx, spec: NetSpec, acc_mode: int = L.ACC_FLOAT, graph_chunk:
 
 
 def compare_batched_looped(ctx, specs: list[NetSpec], steps: int = 1000, acc_mode: int = L.ACC_FLOAT,
-                           graph_chunk: int = 100, tune: bool = True, gen_seed: int = 12345) -> dict:
+                           graph_chunk: int = 100, tune: bool = True, gen_seed: int = 12345,
+                           warmup: int | None = None) -> dict:
     """nets/s of one batched run against the plain path looped per net.
 
     Both sides are timed on the device (CUDA events on the launching stream)
     from the first step to the last, networks already built on the device;
     the looped side is the sum over nets.  Wall-clock times (with a device
     synchronisation at each end) are reported beside them."""
-    batch = Batch(ctx, specs, acc_mode, graph_chunk, gen_seed, tune=tune)
-    batch.run(graph_chunk)  # graph instantiation outside the timed region
+    batch = Batch(ctx, specs, acc_mode, graph_chunk, gen_seed)
+    warm = warmup if warmup is not None else 3 * graph_chunk
+    batch.run(warm)  # graph instantiation and initial transient outside the timed region
     ctx.sync()
+    if tune:  # on the warmed-up network: replays of a representative step
+        from .autotune import tune as _tune
+        _tune(batch.net, replays=20)
+        batch.run(graph_chunk)  # graphs of the chosen shape
+        ctx.sync()
     batch.spikes_per_net(reset=True)
     t0 = time.perf_counter()
     batch.run(steps)
@@ -188,7 +197,7 @@ def compare_batched_looped(ctx, specs: list[NetSpec], steps: int = 1000, acc_mod
     s_loop = np.zeros(len(specs), np.uint64)
     for i, spec in enumerate(specs):
         net = single_network(ctx, spec, acc_mode, graph_chunk, gen_seed)
-        net.run_device(graph_chunk)
+        net.run_device(warm + (graph_chunk if tune else 0))  # same warm-up as the batch
         ctx.sync()
         net.group_spikes(reset=True)
         t0 = time.perf_counter()

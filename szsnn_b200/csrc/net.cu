@@ -21,7 +21,14 @@
 //    ballot and one atomic per spiking warp, raster word written from the
 //    ballot;
 //  * steps captured in CUDA graphs of `chunk` steps; the step counter lives in
-//    device memory, so no host synchronisation happens between steps.
+//    device memory, so no host synchronisation happens between steps;
+//  * overlapped stepping (default): the input arrays are double-buffered by
+//    step parity.  Delivery of delays m >= 2 into step t+1's inputs only
+//    reads ring slots of steps <= t-1, so it runs on a second stream while
+//    update(t) runs; update(t) itself delivers the m = 1 bucket of the units
+//    that spike in it (one warp per spiking warp).  The classic order
+//    (propagate(t) with m = 1..D, then update(t), one buffer) remains
+//    selectable and is what the allocation-free single step uses.
 #include "common.cuh"
 
 #include <cstring>
@@ -46,19 +53,26 @@ struct NetDev {
     const PopDev* pops;
     const unsigned long long* row_ptr;
     const int2* syn;
+    unsigned long long n_syn;  // synapses in syn[] (bounds the L2 prefetches; 0 disables them)
     float* st0;
     float* st1;
     float* st2;
     float* st3;
-    float* in_e;
+    float* in_e;          // parity-0 input buffers (the only ones in classic order)
     float* in_i;
     long long* fx_e;
     long long* fx_i;
+    float* in_e1;         // parity-1 buffers (overlapped stepping)
+    float* in_i1;
+    long long* fx_e1;
+    long long* fx_i1;
+    uint32_t overlap;
     uint32_t acc_mode;
     uint32_t* ring_cnt;
     int32_t* ring_ids;
     const long long* clock;
-    unsigned long long* stats;  // [0] events, [1] spikes (all but the newest step)
+    unsigned long long* stats;  // [0] events consumed, [1] spikes (all but the newest step),
+                                // [2 + p] events delivered into the parity-p buffer, not yet consumed
     uint32_t* err;
     float* dbg_in_e;
     float* dbg_in_i;
@@ -84,21 +98,25 @@ struct szsnn_net {
     unsigned long long* d_row_ptr = nullptr;
     int2* d_syn = nullptr;
     float* d_st[4] = {};
-    float* d_in_e = nullptr;
-    float* d_in_i = nullptr;
-    long long* d_fx_e = nullptr;
-    long long* d_fx_i = nullptr;
+    float* d_in_e[2] = {};       // exc / inh inputs, one buffer per step parity (overlapped stepping)
+    float* d_in_i[2] = {};
+    long long* d_fx_e[2] = {};   // fixed-point inputs (acc_mode FIXED)
+    long long* d_fx_i[2] = {};
     uint32_t* d_ring_cnt = nullptr;
     int32_t* d_ring_ids = nullptr;
     long long* d_clock = nullptr;
     unsigned long long* d_stats = nullptr;
     int chunk = 100;
-    uint32_t* d_forced_stage = nullptr;
+    uint32_t* d_forced_stage[2] = {};   // chunk * words each, alternating chunks
     float* d_current_stage = nullptr;
-    uint32_t* d_raster_stage = nullptr;
+    uint32_t* d_raster_stage[2] = {};
     float* d_dbg_in = nullptr;
-    uint32_t* h_pinned_words = nullptr;  // pinned bounce buffer: chunk * words
-    std::map<std::tuple<int, int>, cudaGraphExec_t> graphs;
+    uint32_t* h_pinned_words = nullptr;  // pinned: one step's words (szsnn_net_step)
+    uint32_t* h_io[4] = {};              // pinned bounce buffers for pageable host arrays: in0, in1, out0, out1
+    cudaStream_t copy_st = nullptr;      // host <-> device copies of szsnn_net_run
+    cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {};
+    bool overlap = true;
+    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;  // (steps, io flags, stage parity)
     int64_t steps_done = 0;
     uint64_t graph_launches = 0, kernel_launches = 0;
     int prop_mode = 0, prop_group = 16, prop_blocks = 0, upd_block = 256;
@@ -133,29 +151,84 @@ __device__ __forceinline__ bool run_neuron(const P& p, int model, uint32_t flags
 
 __global__ void k_advance(long long* clock, int k) { *clock += k; }
 
-template <int G>
-__global__ void __launch_bounds__(256) k_propagate(NetDev nd, int k_off)
+// propagate flags
+#define PF_ZERO_SLOT 1u  // zero the ring count of slot t (classic order: update(t) fills it next)
+#define PF_SPIKES 2u     // add the spike count of step t-1 to the statistics
+#define PF_PENDING 4u    // count events as delivered into the parity buffer of step t, not yet consumed
+
+struct InBuf {
+    float* e;
+    float* i;
+    long long* fe;
+    long long* fi;
+};
+
+// input buffers that step t's update consumes
+__device__ __forceinline__ InBuf in_buf(const NetDev& nd, long long t)
 {
-    __shared__ uint32_t s_pre[1025];
-    __shared__ unsigned long long s_ev;
-    const long long t = *nd.clock + k_off;
+    if (nd.overlap && (t & 1)) return InBuf{nd.in_e1, nd.in_i1, nd.fx_e1, nd.fx_i1};
+    return InBuf{nd.in_e, nd.in_i, nd.fx_e, nd.fx_i};
+}
+
+// one synapse into the exc / inh input of its target (weight sign picks the
+// channel, gather_kernel.cl:172-178; w == 0 is padding and counts nothing)
+__device__ __forceinline__ void deliver(const NetDev& nd, const InBuf& b, int2 sw, uint32_t& ev)
+{
+    const float w = __int_as_float(sw.y);
+    if (w == 0.0f) return;
+    if ((unsigned long long)sw.x >= (unsigned long long)nd.N) {
+        dev_error(nd.err, SZSNN_DEV_BAD_TARGET, (uint32_t)sw.x);
+        return;
+    }
+    ++ev;
+    if (nd.acc_mode == SZSNN_ACC_FIXED) {
+        const long long qv = __float2ll_rn(w * 4294967296.0f);
+        atomicAdd((unsigned long long*)(w >= 0.0f ? &b.fe[sw.x] : &b.fi[sw.x]), (unsigned long long)qv);
+    } else {
+        atomicAdd(w >= 0.0f ? &b.e[sw.x] : &b.i[sw.x], w);
+    }
+}
+
+// Bucket [a, e) of syn[] into L2 ahead of its use (the next step reads the
+// bucket after the one this step reads: a spike's delay buckets are
+// contiguous).  One bulk prefetch per bucket, 16-byte aligned, kept inside the
+// array's first n_syn entries.
+__device__ __forceinline__ void l2_prefetch_bucket(const NetDev& nd, unsigned long long a, unsigned long long e)
+{
+    if (e > nd.n_syn) e = nd.n_syn;
+    if (e <= a) return;
+    const uintptr_t base = (uintptr_t)nd.syn;
+    const uintptr_t lo = (base + a * 8) & ~(uintptr_t)15;
+    uintptr_t hi = (base + e * 8 + 15) & ~(uintptr_t)15;
+    const uintptr_t lim = (base + nd.n_syn * 8) & ~(uintptr_t)15;
+    if (hi > lim) hi = lim;
+    if (hi <= lo) return;
+    const uint32_t bytes = (uint32_t)min((uintptr_t)(hi - lo), (uintptr_t)(1u << 16));
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"(bytes) : "memory");
+}
+
+// ring-slot counts of delays m_lo..D for step t, inclusive scan in s_pre[1..D]
+// (s_pre[0] = 0); block 0 does the slot / statistics bookkeeping of `pf`
+__device__ __forceinline__ void propagate_prologue(const NetDev& nd, long long t, int m_lo, uint32_t pf,
+                                                   uint32_t* s_pre, unsigned long long* s_ev, bool lead)
+{
     const int D = nd.D, R = D + 1;
     for (int m = threadIdx.x + 1; m <= D; m += blockDim.x) {
-        long long tm = t - m;
-        s_pre[m] = (tm >= 0) ? nd.ring_cnt[tm % R] : 0u;
+        const long long tm = t - m;
+        s_pre[m] = (m >= m_lo && tm >= 0) ? nd.ring_cnt[tm % R] : 0u;
     }
-    if (threadIdx.x == 0) { s_pre[0] = 0; s_ev = 0; }
+    if (threadIdx.x == 0) { s_pre[0] = 0; *s_ev = 0; }
     __syncthreads();
     if (threadIdx.x < 32) {  // inclusive scan of counts over m = 1..D
         uint32_t carry = 0;
         const uint32_t lane = threadIdx.x;
         for (int m0 = 1; m0 <= D; m0 += 32) {
-            int m = m0 + (int)lane;
-            uint32_t c = (m <= D) ? s_pre[m] : 0u;
+            const int m = m0 + (int)lane;
+            const uint32_t c = (m <= D) ? s_pre[m] : 0u;
             uint32_t incl = c;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= (uint32_t)o) incl += y;
             }
             if (m <= D) s_pre[m] = carry + incl;
@@ -163,19 +236,44 @@ __global__ void __launch_bounds__(256) k_propagate(NetDev nd, int k_off)
         }
     }
     __syncthreads();
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        nd.ring_cnt[t % R] = 0;                                  // slot filled by update(t)
-        if (t >= 1) atomicAdd(&nd.stats[1], (unsigned long long)(s_pre[1]));  // spikes of step t-1
+    if (lead && threadIdx.x == 0) {
+        if (pf & PF_ZERO_SLOT) nd.ring_cnt[t % R] = 0;  // slot t held step t-R, no longer needed
+        if ((pf & PF_SPIKES) && t >= 1) atomicAdd(&nd.stats[1], (unsigned long long)s_pre[1]);  // step t-1
     }
+}
+
+__device__ __forceinline__ void propagate_epilogue(const NetDev& nd, long long t, uint32_t pf, uint32_t ev,
+                                                   unsigned long long* s_ev)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
+    if ((threadIdx.x & 31) == 0 && ev) atomicAdd(s_ev, (unsigned long long)ev);
+    __syncthreads();
+    if (threadIdx.x == 0 && *s_ev) atomicAdd(&nd.stats[(pf & PF_PENDING) ? 2 + (t & 1) : 0], *s_ev);
+}
+
+// Delivery of ring slots t-m, m = m_lo..D, over bucket m of each spiking unit
+// into step t's inputs: grid-stride over (delay, spike) work items, G lanes
+// per bucket segment.
+// (blk, nblk): this block's index among the nblk blocks doing the delivery
+template <int G>
+__device__ __forceinline__ void propagate_grouped(const NetDev& nd, int k_off, int m_lo, uint32_t pf, int blk, int nblk)
+{
+    __shared__ uint32_t s_pre[1025];
+    __shared__ unsigned long long s_ev;
+    const long long t = *nd.clock + k_off;
+    const int D = nd.D, R = D + 1;
+    propagate_prologue(nd, t, m_lo, pf, s_pre, &s_ev, blk == 0);
+    const InBuf buf = in_buf(nd, t);
     const uint32_t total = s_pre[D];
     const uint32_t lg = threadIdx.x % G;
-    const int64_t gid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
-    const int64_t ngroups = ((int64_t)gridDim.x * blockDim.x) / G;
+    const int64_t gid = ((int64_t)blk * blockDim.x + threadIdx.x) / G;
+    const int64_t ngroups = ((int64_t)nblk * blockDim.x) / G;
     uint32_t ev = 0;
     for (int64_t item = gid; item < (int64_t)total; item += ngroups) {
         int lo = 1, hi = D;  // first m with s_pre[m] > item
         while (lo < hi) {
-            int mid = (lo + hi) >> 1;
+            const int mid = (lo + hi) >> 1;
             if ((int64_t)s_pre[mid] > item) hi = mid; else lo = mid + 1;
         }
         const int m = lo;
@@ -184,31 +282,16 @@ __global__ void __launch_bounds__(256) k_propagate(NetDev nd, int k_off)
         const int64_t s = nd.ring_ids[slot * nd.U + j];
         const unsigned long long a = nd.row_ptr[s * D + (m - 1)];
         const unsigned long long e = nd.row_ptr[s * D + m];
-        for (unsigned long long q = a + lg; q < e; q += G) {
-            const int2 sw = nd.syn[q];
-            const float w = __int_as_float(sw.y);
-            if (w != 0.0f) {
-                if ((unsigned long long)sw.x >= (unsigned long long)nd.N) {
-                    dev_error(nd.err, SZSNN_DEV_BAD_TARGET, (uint32_t)sw.x);
-                    continue;
-                }
-                ++ev;
-                if (nd.acc_mode == SZSNN_ACC_FIXED) {
-                    long long qv = __float2ll_rn(w * 4294967296.0f);
-                    atomicAdd((unsigned long long*)(w >= 0.0f ? &nd.fx_e[sw.x] : &nd.fx_i[sw.x]),
-                              (unsigned long long)qv);
-                } else {
-                    atomicAdd(w >= 0.0f ? &nd.in_e[sw.x] : &nd.in_i[sw.x], w);
-                }
-            }
-        }
+        if (lg == 0 && m < D) l2_prefetch_bucket(nd, e, nd.row_ptr[s * D + m + 1]);  // bucket m+1: next step
+        for (unsigned long long q = a + lg; q < e; q += G) deliver(nd, buf, nd.syn[q], ev);
     }
-    // events: warp reduce, one shared atomic per warp, one global per block
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
-    if ((threadIdx.x & 31) == 0 && ev) atomicAdd(&s_ev, (unsigned long long)ev);
-    __syncthreads();
-    if (threadIdx.x == 0 && s_ev) atomicAdd(&nd.stats[0], s_ev);
+    propagate_epilogue(nd, t, pf, ev, &s_ev);
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) k_propagate(NetDev nd, int k_off, int m_lo, uint32_t pf)
+{
+    propagate_grouped<G>(nd, k_off, m_lo, pf, blockIdx.x, gridDim.x);
 }
 
 // Warp-flattened delivery: lanes 0..IPW-1 each resolve one (delay, spike)
@@ -217,43 +300,19 @@ __global__ void __launch_bounds__(256) k_propagate(NetDev nd, int k_off)
 // search over the lanes' exclusive offsets with shuffles), UNR loads in
 // flight per lane before their atomics.
 template <int IPW>
-__global__ void __launch_bounds__(256) k_propagate_flat(NetDev nd, int k_off)
+__device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int m_lo, uint32_t pf, int blk, int nblk)
 {
     constexpr int UNR = 4;
     __shared__ uint32_t s_pre[1025];
     __shared__ unsigned long long s_ev;
     const long long t = *nd.clock + k_off;
     const int D = nd.D, R = D + 1;
-    for (int m = threadIdx.x + 1; m <= D; m += blockDim.x) {
-        long long tm = t - m;
-        s_pre[m] = (tm >= 0) ? nd.ring_cnt[tm % R] : 0u;
-    }
-    if (threadIdx.x == 0) { s_pre[0] = 0; s_ev = 0; }
-    __syncthreads();
+    propagate_prologue(nd, t, m_lo, pf, s_pre, &s_ev, blk == 0);
+    const InBuf buf = in_buf(nd, t);
     const uint32_t lane = threadIdx.x & 31;
-    if (threadIdx.x < 32) {
-        uint32_t carry = 0;
-        for (int m0 = 1; m0 <= D; m0 += 32) {
-            int m = m0 + (int)lane;
-            uint32_t c = (m <= D) ? s_pre[m] : 0u;
-            uint32_t incl = c;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= (uint32_t)o) incl += y;
-            }
-            if (m <= D) s_pre[m] = carry + incl;
-            carry += __shfl_sync(0xffffffffu, incl, 31);
-        }
-    }
-    __syncthreads();
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        nd.ring_cnt[t % R] = 0;
-        if (t >= 1) atomicAdd(&nd.stats[1], (unsigned long long)(s_pre[1]));
-    }
     const uint32_t total = s_pre[D];
-    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t gw = ((int64_t)blk * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)nblk * blockDim.x) >> 5;
     const int2* __restrict__ syn = nd.syn;
     uint32_t ev = 0;
     for (int64_t base = gw * IPW; base < (int64_t)total; base += nw * IPW) {
@@ -262,7 +321,7 @@ __global__ void __launch_bounds__(256) k_propagate_flat(NetDev nd, int k_off)
         if (lane < (uint32_t)IPW && item < (int64_t)total) {
             int lo = 1, hi = D;
             while (lo < hi) {
-                int mid = (lo + hi) >> 1;
+                const int mid = (lo + hi) >> 1;
                 if ((int64_t)s_pre[mid] > item) hi = mid; else lo = mid + 1;
             }
             const int m = lo;
@@ -270,12 +329,13 @@ __global__ void __launch_bounds__(256) k_propagate_flat(NetDev nd, int k_off)
             const int64_t s = __ldg(&nd.ring_ids[((t - m) % R) * nd.U + j]);
             a = __ldg(&nd.row_ptr[s * D + (m - 1)]);
             e = __ldg(&nd.row_ptr[s * D + m]);
+            if (m < D) l2_prefetch_bucket(nd, e, __ldg(&nd.row_ptr[s * D + m + 1]));  // bucket m+1: next step
         }
         const uint32_t len = (uint32_t)(e - a);
         uint32_t incl = len;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= (uint32_t)o) incl += y;
         }
         const uint32_t excl = incl - len;
@@ -299,30 +359,17 @@ __global__ void __launch_bounds__(256) k_propagate_flat(NetDev nd, int k_off)
                 sw[u] = ok[u] ? __ldg(&syn[oa + (k - oex)]) : make_int2(0, 0);
             }
 #pragma unroll
-            for (int u = 0; u < UNR; ++u) {
-                const float w = __int_as_float(sw[u].y);
-                if (ok[u] && w != 0.0f) {
-                    if ((unsigned long long)sw[u].x >= (unsigned long long)nd.N) {
-                        dev_error(nd.err, SZSNN_DEV_BAD_TARGET, (uint32_t)sw[u].x);
-                        continue;
-                    }
-                    ++ev;
-                    if (nd.acc_mode == SZSNN_ACC_FIXED) {
-                        long long qv = __float2ll_rn(w * 4294967296.0f);
-                        atomicAdd((unsigned long long*)(w >= 0.0f ? &nd.fx_e[sw[u].x] : &nd.fx_i[sw[u].x]),
-                                  (unsigned long long)qv);
-                    } else {
-                        atomicAdd(w >= 0.0f ? &nd.in_e[sw[u].x] : &nd.in_i[sw[u].x], w);
-                    }
-                }
-            }
+            for (int u = 0; u < UNR; ++u)
+                if (ok[u]) deliver(nd, buf, sw[u], ev);
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
-    if (lane == 0 && ev) atomicAdd(&s_ev, (unsigned long long)ev);
-    __syncthreads();
-    if (threadIdx.x == 0 && s_ev) atomicAdd(&nd.stats[0], s_ev);
+    propagate_epilogue(nd, t, pf, ev, &s_ev);
+}
+
+template <int IPW>
+__global__ void __launch_bounds__(256) k_propagate_flat(NetDev nd, int k_off, int m_lo, uint32_t pf)
+{
+    propagate_flat<IPW>(nd, k_off, m_lo, pf, blockIdx.x, gridDim.x);
 }
 
 // last population with begin <= id, or -1 (ranges sorted and disjoint)
@@ -342,20 +389,25 @@ __device__ __forceinline__ int find_pop(const PopDev* pops, int npops, int64_t i
 // block (and the step counter) in shared memory while every thread already
 // has its state loads in flight, so each thread's chain of dependent global
 // accesses is: state / input loads -> model arithmetic -> stores.
-__global__ void __launch_bounds__(1024) k_update(NetDev nd, int k_off, const uint32_t* __restrict__ forced,
-                                                const float* __restrict__ current, uint32_t* __restrict__ out_words)
+// Overlapped stepping: the inputs of step t are the parity buffer of t; the
+// warps with spikes deliver their units' m = 1 buckets into the buffer of
+// t+1, and block 0 does the per-step bookkeeping (spikes of step t-1 into the
+// statistics, slot t+1 emptied for update(t+1), events of step t's buffer
+// moved from pending to consumed).
+__device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk, const uint32_t* __restrict__ forced,
+                                            const float* __restrict__ current, uint32_t* __restrict__ out_words)
 {
     __shared__ PopDev s_pop[UPD_BLOCK_POPS];
     __shared__ int s_np;  // populations staged, -1 when more overlap the block (global lookup)
     __shared__ long long s_t;
-    const int64_t b0 = (int64_t)blockIdx.x * blockDim.x;
+    const int64_t b0 = (int64_t)blk * blockDim.x;
     const int64_t id = b0 + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31;
     // populations overlapping the block: the whole table when it is small, else
     // the host-computed (first, count) of this block; one cooperative copy
     int first = 0, np = nd.npops;
     if (np > UPD_BLOCK_POPS) {
-        const int2 fc = nd.blk_pop[blockIdx.x];
+        const int2 fc = nd.blk_pop[blk];
         first = fc.x;
         np = fc.y > UPD_BLOCK_POPS ? -1 : fc.y;
     }
@@ -365,6 +417,8 @@ __global__ void __launch_bounds__(1024) k_update(NetDev nd, int k_off, const uin
         for (int w = threadIdx.x; w < np * (int)(sizeof(PopDev) / 8); w += blockDim.x) dst[w] = src[w];
     }
     if (threadIdx.x == 0) { s_np = np; s_t = *nd.clock + k_off; }
+    const int64_t tq = (int64_t)(*nd.clock + k_off);  // all threads: selects the input buffer
+    const InBuf inb = in_buf(nd, tq);
     float* __restrict__ st0 = nd.st0;
     float* __restrict__ st1 = nd.st1;
     float* __restrict__ st2 = nd.st2;
@@ -377,13 +431,21 @@ __global__ void __launch_bounds__(1024) k_update(NetDev nd, int k_off, const uin
         g1 = st1[id];
         g2 = st2[id];
         fr = st3[id];
-        if (nd.acc_mode == SZSNN_ACC_FIXED) { fxe = nd.fx_e[id]; fxi = nd.fx_i[id]; }
-        else { in_e = nd.in_e[id]; in_i = nd.in_i[id]; }
+        if (nd.acc_mode == SZSNN_ACC_FIXED) { fxe = inb.fe[id]; fxi = inb.fi[id]; }
+        else { in_e = inb.e[id]; in_i = inb.i[id]; }
         if (current) i_ext = current[id];
     }
     const bool f = (forced && unit) ? ((forced[id >> 5] >> (id & 31)) & 1u) : false;
     __syncthreads();
     const long long t = s_t;
+    if (nd.overlap && blk == 0 && threadIdx.x == 0) {
+        const int R = nd.D + 1;
+        if (t >= 1) atomicAdd(&nd.stats[1], (unsigned long long)nd.ring_cnt[(t - 1) % R]);
+        nd.ring_cnt[(t + 1) % R] = 0;  // held step t-D, read last by the delivery into step t
+        const unsigned long long pend = nd.stats[2 + (t & 1)];
+        nd.stats[2 + (t & 1)] = 0;
+        atomicAdd(&nd.stats[0], pend);
+    }
     const PopDev* pd = nullptr;
     if (unit) {
         const int np = s_np;
@@ -402,11 +464,11 @@ __global__ void __launch_bounds__(1024) k_update(NetDev nd, int k_off, const uin
             if (nd.acc_mode == SZSNN_ACC_FIXED) {
                 in_e = __ll2float_rn(fxe) * (1.0f / 4294967296.0f);
                 in_i = __ll2float_rn(fxi) * (1.0f / 4294967296.0f);
-                nd.fx_e[id] = 0;
-                nd.fx_i[id] = 0;
+                inb.fe[id] = 0;
+                inb.fi[id] = 0;
             } else {
-                nd.in_e[id] = 0.0f;
-                nd.in_i[id] = 0.0f;
+                inb.e[id] = 0.0f;
+                inb.i[id] = 0.0f;
             }
             if (nd.dbg_in_e) { nd.dbg_in_e[id] = in_e; nd.dbg_in_i[id] = in_i; }
             if (pd->pn) spk = run_neuron(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, model, pd->flags,
@@ -440,7 +502,49 @@ __global__ void __launch_bounds__(1024) k_update(NetDev nd, int k_off, const uin
             if (pos < (uint32_t)nd.U) nd.ring_ids[slot * nd.U + pos] = (int32_t)id;
             else dev_error(nd.err, SZSNN_DEV_RING_OVERFLOW, (uint32_t)slot);
         }
+        if (nd.overlap) {  // m = 1 buckets of this warp's spiking units into step t+1's inputs
+            const InBuf nb = in_buf(nd, t + 1);
+            unsigned long long ra = 0, re = 0;
+            if (spk) {
+                ra = nd.row_ptr[id * nd.D];
+                re = nd.row_ptr[id * nd.D + 1];
+                if (nd.D >= 2) l2_prefetch_bucket(nd, re, nd.row_ptr[id * nd.D + 2]);  // bucket 2: step t+2
+            }
+            uint32_t ev = 0;
+            for (uint32_t bits = ball; bits; bits &= bits - 1u) {
+                const int l = __ffs(bits) - 1;
+                const unsigned long long a = __shfl_sync(0xffffffffu, ra, l);
+                const unsigned long long e = __shfl_sync(0xffffffffu, re, l);
+                for (unsigned long long q = a + lane; q < e; q += 32) deliver(nd, nb, nd.syn[q], ev);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
+            if (lane == 0 && ev) atomicAdd(&nd.stats[2 + ((t + 1) & 1)], (unsigned long long)ev);
+        }
     }
+}
+
+__global__ void __launch_bounds__(1024) k_update(NetDev nd, int k_off, const uint32_t* __restrict__ forced,
+                                                const float* __restrict__ current, uint32_t* __restrict__ out_words)
+{
+    update_body(nd, k_off, blockIdx.x, forced, current, out_words);
+}
+
+// Overlapped step t in one launch: blocks 0..far_blocks-1 deliver delays >= 2
+// into step t+1's inputs (reading ring slots <= t-1 only), the others update
+// step t (which delivers its own spikes' delay-1 buckets into step t+1).  The
+// delivery blocks come first so they are resident from the start and run
+// beside the update blocks.
+template <int G>
+__global__ void __launch_bounds__(1024) k_step(NetDev nd, int k_off, int far_blocks, const uint32_t* __restrict__ forced,
+                                              const float* __restrict__ current, uint32_t* __restrict__ out_words)
+{
+    if ((int)blockIdx.x < far_blocks) {  // G > 0: grouped delivery, G lanes per bucket; G < 0: flattened, -G items per warp
+        if constexpr (G > 0) propagate_grouped<G>(nd, k_off + 1, 2, PF_PENDING, blockIdx.x, far_blocks);
+        else propagate_flat<-G>(nd, k_off + 1, 2, PF_PENDING, blockIdx.x, far_blocks);
+        return;
+    }
+    update_body(nd, k_off, blockIdx.x - far_blocks, forced, current, out_words);
 }
 
 // ---- device generator (fixed fan-out), one warp per row
@@ -561,9 +665,11 @@ NetDev make_dev(szsnn_net* n)
 {
     NetDev d{};
     d.N = n->N; d.U = n->U; d.words = n->words; d.D = n->D; d.npops = n->npops;
-    d.pops = n->d_pops; d.row_ptr = n->d_row_ptr; d.syn = n->d_syn;
+    d.pops = n->d_pops; d.row_ptr = n->d_row_ptr; d.syn = n->d_syn; d.n_syn = n->n_syn;
     d.st0 = n->d_st[0]; d.st1 = n->d_st[1]; d.st2 = n->d_st[2]; d.st3 = n->d_st[3];
-    d.in_e = n->d_in_e; d.in_i = n->d_in_i; d.fx_e = n->d_fx_e; d.fx_i = n->d_fx_i;
+    d.in_e = n->d_in_e[0]; d.in_i = n->d_in_i[0]; d.fx_e = n->d_fx_e[0]; d.fx_i = n->d_fx_i[0];
+    d.in_e1 = n->d_in_e[1]; d.in_i1 = n->d_in_i[1]; d.fx_e1 = n->d_fx_e[1]; d.fx_i1 = n->d_fx_i[1];
+    d.overlap = n->overlap ? 1u : 0u;
     d.acc_mode = n->acc_mode; d.ring_cnt = n->d_ring_cnt; d.ring_ids = n->d_ring_ids;
     d.clock = n->d_clock; d.stats = n->d_stats; d.err = n->ctx->d_err;
     d.dbg_in_e = nullptr; d.dbg_in_i = nullptr;
@@ -572,25 +678,38 @@ NetDev make_dev(szsnn_net* n)
     return d;
 }
 
-cudaError_t launch_propagate(szsnn_net* n, const NetDev& d, int k_off)
+// delivery of delays m_lo..D into the inputs of step clock + k_off
+cudaError_t launch_propagate(szsnn_net* n, const NetDev& d, int k_off, int m_lo, uint32_t pf, cudaStream_t st)
 {
     int blocks = n->prop_blocks > 0 ? n->prop_blocks : num_sms(n->ctx) * 16;
-    cudaStream_t st = n->ctx->stream;
     if (n->prop_mode == 1) {
         switch (n->prop_group) {
-        case 8: k_propagate_flat<8><<<blocks, 256, 0, st>>>(d, k_off); break;
-        case 16: k_propagate_flat<16><<<blocks, 256, 0, st>>>(d, k_off); break;
-        default: k_propagate_flat<32><<<blocks, 256, 0, st>>>(d, k_off); break;
+        case 8: k_propagate_flat<8><<<blocks, 256, 0, st>>>(d, k_off, m_lo, pf); break;
+        case 16: k_propagate_flat<16><<<blocks, 256, 0, st>>>(d, k_off, m_lo, pf); break;
+        default: k_propagate_flat<32><<<blocks, 256, 0, st>>>(d, k_off, m_lo, pf); break;
         }
         return cudaGetLastError();
     }
     switch (n->prop_group) {
-    case 4: k_propagate<4><<<blocks, 256, 0, st>>>(d, k_off); break;
-    case 8: k_propagate<8><<<blocks, 256, 0, st>>>(d, k_off); break;
-    case 32: k_propagate<32><<<blocks, 256, 0, st>>>(d, k_off); break;
-    default: k_propagate<16><<<blocks, 256, 0, st>>>(d, k_off); break;
+    case 4: k_propagate<4><<<blocks, 256, 0, st>>>(d, k_off, m_lo, pf); break;
+    case 8: k_propagate<8><<<blocks, 256, 0, st>>>(d, k_off, m_lo, pf); break;
+    case 32: k_propagate<32><<<blocks, 256, 0, st>>>(d, k_off, m_lo, pf); break;
+    default: k_propagate<16><<<blocks, 256, 0, st>>>(d, k_off, m_lo, pf); break;
     }
     return cudaGetLastError();
+}
+
+// classic order: all delays into step t's (single) buffer, slot t emptied
+cudaError_t launch_propagate_classic(szsnn_net* n, const NetDev& d, int k_off, cudaStream_t st)
+{
+    return launch_propagate(n, d, k_off, 1, PF_ZERO_SLOT | PF_SPIKES, st);
+}
+
+// overlapped order: delays 2..D into the parity buffer of step clock + k_off
+cudaError_t launch_propagate_far(szsnn_net* n, const NetDev& d, int k_off, cudaStream_t st)
+{
+    if (n->D < 2) return cudaSuccess;
+    return launch_propagate(n, d, k_off, 2, PF_PENDING, st);
 }
 
 // (first pop, count) overlapping each update block of `bs` threads
@@ -618,11 +737,36 @@ cudaError_t fill_blk_pop(szsnn_net* n)
 }
 
 cudaError_t launch_update(szsnn_net* n, const NetDev& d, int k_off, const uint32_t* forced, const float* cur,
-                          uint32_t* words)
+                          uint32_t* words, cudaStream_t st)
 {
     int bs = n->upd_block;
     int64_t blocks = sz_div_up(n->U, bs);
-    k_update<<<(unsigned)blocks, bs, 0, n->ctx->stream>>>(d, k_off, forced, cur, words);
+    k_update<<<(unsigned)blocks, bs, 0, st>>>(d, k_off, forced, cur, words);
+    return cudaGetLastError();
+}
+
+// overlapped step clock + k_off: far delivery into step t+1 and update(t) in one launch
+cudaError_t launch_step(szsnn_net* n, const NetDev& d, int k_off, const uint32_t* forced, const float* cur,
+                        uint32_t* words, cudaStream_t st)
+{
+    const int bs = n->upd_block;
+    const int far = n->D < 2 ? 0 : (n->prop_blocks > 0 ? n->prop_blocks : num_sms(n->ctx) * std::max(1, 1024 / bs));
+    const int64_t blocks = far + sz_div_up(n->U, bs);
+    const dim3 grid((unsigned)blocks);
+    if (n->prop_mode == 1) {
+        switch (n->prop_group) {
+        case 8: k_step<-8><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
+        case 16: k_step<-16><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
+        default: k_step<-32><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
+        }
+        return cudaGetLastError();
+    }
+    switch (n->prop_group) {
+    case 4: k_step<4><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
+    case 8: k_step<8><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
+    case 32: k_step<32><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
+    default: k_step<16><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
+    }
     return cudaGetLastError();
 }
 
@@ -647,21 +791,27 @@ void free_net(szsnn_net* n)
     cudaFree(n->d_row_ptr);
     cudaFree(n->d_syn);
     for (int k = 0; k < 4; ++k) cudaFree(n->d_st[k]);
-    cudaFree(n->d_in_e);
-    cudaFree(n->d_in_i);
-    cudaFree(n->d_fx_e);
-    cudaFree(n->d_fx_i);
+    for (int p = 0; p < 2; ++p) {
+        cudaFree(n->d_in_e[p]);
+        cudaFree(n->d_in_i[p]);
+        cudaFree(n->d_fx_e[p]);
+        cudaFree(n->d_fx_i[p]);
+        cudaFree(n->d_forced_stage[p]);
+        cudaFree(n->d_raster_stage[p]);
+    }
     cudaFree(n->d_ring_cnt);
     cudaFree(n->d_ring_ids);
     cudaFree(n->d_clock);
     cudaFree(n->d_stats);
-    cudaFree(n->d_forced_stage);
     cudaFree(n->d_current_stage);
-    cudaFree(n->d_raster_stage);
     cudaFree(n->d_dbg_in);
     if (n->h_pinned_words) cudaFreeHost(n->h_pinned_words);
+    for (auto& h : n->h_io) if (h) cudaFreeHost(h);
     if (n->ev_run0) cudaEventDestroy(n->ev_run0);
     if (n->ev_run1) cudaEventDestroy(n->ev_run1);
+    for (int p = 0; p < 2; ++p)
+        for (cudaEvent_t ev : {n->ev_in[p], n->ev_comp[p], n->ev_out[p]}) if (ev) cudaEventDestroy(ev);
+    if (n->copy_st) cudaStreamDestroy(n->copy_st);
     delete n;
 }
 
@@ -810,23 +960,34 @@ extern "C" int szsnn_net_create(szsnn_ctx* ctx, const szsnn_net_desc* d, szsnn_n
         if (d->state_host[k]) C(cudaMemcpyAsync(n->d_st[k], d->state_host[k], (size_t)U * 4, cudaMemcpyHostToDevice, st));
         else C(cudaMemsetAsync(n->d_st[k], 0, (size_t)U * 4, st));
     }
-    C(dalloc(&n->d_in_e, (size_t)N)); C(cudaMemsetAsync(n->d_in_e, 0, (size_t)std::max<int64_t>(N, 1) * 4, st));
-    C(dalloc(&n->d_in_i, (size_t)N)); C(cudaMemsetAsync(n->d_in_i, 0, (size_t)std::max<int64_t>(N, 1) * 4, st));
-    if (n->acc_mode == SZSNN_ACC_FIXED) {
-        C(dalloc(&n->d_fx_e, (size_t)N)); C(cudaMemsetAsync(n->d_fx_e, 0, (size_t)std::max<int64_t>(N, 1) * 8, st));
-        C(dalloc(&n->d_fx_i, (size_t)N)); C(cudaMemsetAsync(n->d_fx_i, 0, (size_t)std::max<int64_t>(N, 1) * 8, st));
+    const size_t N1 = (size_t)std::max<int64_t>(N, 1);
+    for (int p = 0; p < 2; ++p) {
+        C(dalloc(&n->d_in_e[p], N1)); C(cudaMemsetAsync(n->d_in_e[p], 0, N1 * 4, st));
+        C(dalloc(&n->d_in_i[p], N1)); C(cudaMemsetAsync(n->d_in_i[p], 0, N1 * 4, st));
+        if (n->acc_mode == SZSNN_ACC_FIXED) {
+            C(dalloc(&n->d_fx_e[p], N1)); C(cudaMemsetAsync(n->d_fx_e[p], 0, N1 * 8, st));
+            C(dalloc(&n->d_fx_i[p], N1)); C(cudaMemsetAsync(n->d_fx_i[p], 0, N1 * 8, st));
+        }
     }
     C(dalloc(&n->d_ring_cnt, (size_t)n->R)); C(cudaMemsetAsync(n->d_ring_cnt, 0, (size_t)n->R * 4, st));
     C(dalloc(&n->d_ring_ids, (size_t)n->R * U));
     C(dalloc(&n->d_clock, 1)); C(cudaMemsetAsync(n->d_clock, 0, 8, st));
     C(dalloc(&n->d_stats, 4)); C(cudaMemsetAsync(n->d_stats, 0, 32, st));
-    C(dalloc(&n->d_forced_stage, (size_t)n->chunk * n->words));
+    for (int p = 0; p < 2; ++p) {
+        C(dalloc(&n->d_forced_stage[p], (size_t)n->chunk * n->words));
+        C(dalloc(&n->d_raster_stage[p], (size_t)n->chunk * n->words));
+    }
     C(dalloc(&n->d_current_stage, (size_t)n->chunk * std::max<int64_t>(N, 1)));
-    C(dalloc(&n->d_raster_stage, (size_t)n->chunk * n->words));
     C(dalloc(&n->d_dbg_in, (size_t)2 * std::max<int64_t>(N, 1)));
-    C(cudaMallocHost((void**)&n->h_pinned_words, (size_t)n->chunk * n->words * 4));
+    C(cudaMallocHost((void**)&n->h_pinned_words, (size_t)n->words * 4));
     C(cudaEventCreate(&n->ev_run0));
     C(cudaEventCreate(&n->ev_run1));
+    C(cudaStreamCreateWithFlags(&n->copy_st, cudaStreamNonBlocking));
+    for (int p = 0; p < 2; ++p) {
+        C(cudaEventCreateWithFlags(&n->ev_in[p], cudaEventDisableTiming));
+        C(cudaEventCreateWithFlags(&n->ev_comp[p], cudaEventDisableTiming));
+        C(cudaEventCreateWithFlags(&n->ev_out[p], cudaEventDisableTiming));
+    }
     C(cudaStreamSynchronize(st));
 #undef C
     *out = n;
@@ -868,6 +1029,8 @@ extern "C" int szsnn_net_generate(szsnn_net* n, const szsnn_gen_block* blocks, i
     }
     if (off != n->n_syn) {  // (re)allocate synapse storage for the generated count
         NET_TRY(n, cudaStreamSynchronize(st));
+        for (auto& kv : n->graphs) cudaGraphExecDestroy(kv.second);  // they hold the old array
+        n->graphs.clear();
         cudaFree(n->d_syn);
         n->d_syn = nullptr;
         NET_TRY(n, dalloc(&n->d_syn, (size_t)off));
@@ -899,7 +1062,7 @@ static int net_stage_step_inputs(szsnn_net* n, const uint32_t* forced_host, cons
 {
     cudaStream_t st = n->ctx->stream;
     if (forced_host)
-        NET_TRY(n, cudaMemcpyAsync(n->d_forced_stage, forced_host, (size_t)n->words * 4, cudaMemcpyHostToDevice, st));
+        NET_TRY(n, cudaMemcpyAsync(n->d_forced_stage[0], forced_host, (size_t)n->words * 4, cudaMemcpyHostToDevice, st));
     if (current_host && n->N)
         NET_TRY(n, cudaMemcpyAsync(n->d_current_stage, current_host, (size_t)n->N * 4, cudaMemcpyHostToDevice, st));
     return SZSNN_OK;
@@ -915,25 +1078,33 @@ extern "C" int szsnn_net_step(szsnn_net* n, const uint32_t* forced_host, const f
     d.dbg_in_e = n->d_dbg_in;
     d.dbg_in_i = n->d_dbg_in + std::max<int64_t>(n->N, 1);
     cudaStream_t st = n->ctx->stream;
-    NET_TRY(n, launch_propagate(n, d, 0));
-    NET_TRY(n, launch_update(n, d, 0, forced_host ? n->d_forced_stage : nullptr,
-                             current_host ? n->d_current_stage : nullptr, n->d_raster_stage));
+    const uint32_t* forced = forced_host ? n->d_forced_stage[0] : nullptr;
+    const float* cur = current_host ? n->d_current_stage : nullptr;
+    if (n->overlap) {  // update(t) with its m = 1 deliveries, and delays >= 2 into step t+1
+        NET_TRY(n, launch_step(n, d, 0, forced, cur, n->d_raster_stage[0], st));
+    } else {
+        NET_TRY(n, launch_propagate_classic(n, d, 0, st));
+        NET_TRY(n, launch_update(n, d, 0, forced, cur, n->d_raster_stage[0], st));
+    }
     k_advance<<<1, 1, 0, st>>>(n->d_clock, 1);
     NET_TRY(n, cudaGetLastError());
-    n->kernel_launches += 3;
+    n->kernel_launches += n->overlap ? 2 : 3;
     n->steps_done += 1;
     if (fired_host) {
-        NET_TRY(n, cudaMemcpyAsync(n->h_pinned_words, n->d_raster_stage, (size_t)n->words * 4, cudaMemcpyDeviceToHost, st));
+        NET_TRY(n, cudaMemcpyAsync(n->h_pinned_words, n->d_raster_stage[0], (size_t)n->words * 4, cudaMemcpyDeviceToHost, st));
         NET_TRY(n, cudaStreamSynchronize(st));
         std::memcpy(fired_host, n->h_pinned_words, (size_t)n->words * 4);
     }
     return SZSNN_OK;
 }
 
-// graph of `len` steps; flags bit0 forced, bit1 current, bit2 raster
-static int net_graph(szsnn_net* n, int len, int flags, cudaGraphExec_t* out)
+// graph of `len` steps; flags bit0 forced, bit1 current, bit2 raster; `b`
+// selects the forced / raster stage buffers.  Overlapped order: one k_step
+// per step (on entry the inputs of the first step are complete: its far
+// delivery ran in the previous step's launch, or at priming).
+static int net_graph(szsnn_net* n, int len, int flags, int b, cudaGraphExec_t* out)
 {
-    auto key = std::make_tuple(len, flags);
+    auto key = std::make_tuple(len, flags, b);
     auto it = n->graphs.find(key);
     if (it != n->graphs.end()) { *out = it->second; return SZSNN_OK; }
     cudaStream_t st = n->ctx->stream;
@@ -942,11 +1113,15 @@ static int net_graph(szsnn_net* n, int len, int flags, cudaGraphExec_t* out)
     NET_TRY(n, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < len && e == cudaSuccess; ++k) {
-        e = launch_propagate(n, d, k);
-        if (e != cudaSuccess) break;
-        e = launch_update(n, d, k, (flags & 1) ? n->d_forced_stage + (size_t)k * n->words : nullptr,
-                          (flags & 2) ? n->d_current_stage + (size_t)k * std::max<int64_t>(n->N, 1) : nullptr,
-                          (flags & 4) ? n->d_raster_stage + (size_t)k * n->words : nullptr);
+        const uint32_t* fw = (flags & 1) ? n->d_forced_stage[b] + (size_t)k * n->words : nullptr;
+        const float* cu = (flags & 2) ? n->d_current_stage + (size_t)k * std::max<int64_t>(n->N, 1) : nullptr;
+        uint32_t* ras = (flags & 4) ? n->d_raster_stage[b] + (size_t)k * n->words : nullptr;
+        if (n->overlap) {
+            e = launch_step(n, d, k, fw, cu, ras, st);
+        } else {
+            e = launch_propagate_classic(n, d, k, st);
+            if (e == cudaSuccess) e = launch_update(n, d, k, fw, cu, ras, st);
+        }
     }
     if (e == cudaSuccess) {
         k_advance<<<1, 1, 0, st>>>(n->d_clock, len);
@@ -967,50 +1142,135 @@ static int net_graph(szsnn_net* n, int len, int flags, cudaGraphExec_t* out)
     return SZSNN_OK;
 }
 
+// Inputs of the next step rebuilt from the ring: both buffers and the pending
+// event counters zeroed; in overlapped order all delays (1..D) of step t are
+// then delivered into its parity buffer (what far(t) and update(t-1) would
+// have delivered), slot t emptied, events counted as pending.  Used after a
+// restore and when the step order changes.
+static int net_prime(szsnn_net* n)
+{
+    cudaStream_t st = n->ctx->stream;
+    const size_t N1 = (size_t)std::max<int64_t>(n->N, 1);
+    for (int p = 0; p < 2; ++p) {
+        NET_TRY(n, cudaMemsetAsync(n->d_in_e[p], 0, N1 * 4, st));
+        NET_TRY(n, cudaMemsetAsync(n->d_in_i[p], 0, N1 * 4, st));
+        if (n->d_fx_e[p]) NET_TRY(n, cudaMemsetAsync(n->d_fx_e[p], 0, N1 * 8, st));
+        if (n->d_fx_i[p]) NET_TRY(n, cudaMemsetAsync(n->d_fx_i[p], 0, N1 * 8, st));
+    }
+    NET_TRY(n, cudaMemsetAsync(n->d_stats + 2, 0, 16, st));
+    if (n->overlap) NET_TRY(n, launch_propagate(n, make_dev(n), 0, 1, PF_ZERO_SLOT | PF_PENDING, st));
+    NET_TRY(n, cudaStreamSynchronize(st));
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_set_overlap(szsnn_net* n, int on)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    if (on != 0 && on != 1) return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "overlap must be 0 or 1");
+    if ((on != 0) == n->overlap) return SZSNN_OK;
+    n->overlap = on != 0;
+    for (auto& kv : n->graphs) cudaGraphExecDestroy(kv.second);
+    n->graphs.clear();
+    return net_prime(n);
+}
+
+// true when [p, p + bytes) lies in page-locked host memory (so it can be a
+// DMA source / destination without a bounce copy)
+static bool host_pinned(const void* p, size_t bytes)
+{
+    if (!p || !bytes) return false;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    if (a.type != cudaMemoryTypeHost) return false;
+    cudaPointerAttributes z{};
+    if (cudaPointerGetAttributes(&z, (const char*)p + bytes - 1) != cudaSuccess) { cudaGetLastError(); return false; }
+    return z.type == cudaMemoryTypeHost;
+}
+
+// Chunks of `chunk` steps, each one graph launch.  Host / device copies of the
+// forced words and the raster run on the copy stream into alternating stage
+// buffers, so chunk k's copies overlap chunk k-1's / k+1's compute.  Pinned
+// host arrays are copied directly; pageable ones go through pinned bounce
+// buffers (the copy-out of chunk k to the caller's array happens while chunk
+// k+1 runs).
 static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, const float* current, uint32_t* raster,
                         bool host)
 {
     if (!n || steps < 0) return SZSNN_ERR_ARG;
-    cudaStream_t st = n->ctx->stream;
+    cudaStream_t st = n->ctx->stream, cp = n->copy_st;
+    const size_t wbytes = (size_t)n->words * 4;
+    const bool pin_in = host && forced && host_pinned(forced, (size_t)steps * wbytes);
+    const bool pin_out = host && raster && host_pinned(raster, (size_t)steps * wbytes);
+    const bool bounce_in = host && forced && !pin_in, bounce_out = host && raster && !pin_out;
+    for (int q = 0; q < 4; ++q) {
+        const bool need = q < 2 ? bounce_in : bounce_out;
+        if (need && !n->h_io[q]) NET_TRY(n, cudaMallocHost((void**)&n->h_io[q], (size_t)n->chunk * wbytes));
+    }
     NET_TRY(n, cudaEventRecord(n->ev_run0, st));
+    NET_TRY(n, cudaStreamWaitEvent(cp, n->ev_run0, 0));  // copies follow earlier work on the main stream
     const cudaMemcpyKind in_kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-    for (int64_t done = 0; done < steps;) {
+    const cudaMemcpyKind out_kind = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    struct Pending { bool on; size_t off, bytes; };
+    Pending pend[2] = {{false, 0, 0}, {false, 0, 0}};
+    auto flush = [&](int b) -> int {  // pageable copy-out of the chunk held in bounce buffer b
+        if (!pend[b].on) return SZSNN_OK;
+        NET_TRY(n, cudaEventSynchronize(n->ev_out[b]));
+        std::memcpy((char*)raster + pend[b].off, n->h_io[2 + b], pend[b].bytes);
+        pend[b].on = false;
+        return SZSNN_OK;
+    };
+    int64_t k = 0;
+    for (int64_t done = 0; done < steps; ++k) {
+        const int b = (int)(k & 1);
         const int len = (int)std::min<int64_t>(n->chunk, steps - done);
         const int flags = (forced ? 1 : 0) | (current ? 2 : 0) | (raster ? 4 : 0);
+        const size_t bytes = (size_t)len * wbytes, off = (size_t)done * wbytes;
         if (forced) {
-            const size_t bytes = (size_t)len * n->words * 4;
-            if (host) {  // through the pinned bounce buffer so the copy is a true async DMA
-                NET_TRY(n, cudaStreamSynchronize(st));
-                std::memcpy(n->h_pinned_words, forced + (size_t)done * n->words, bytes);
-                NET_TRY(n, cudaMemcpyAsync(n->d_forced_stage, n->h_pinned_words, bytes, cudaMemcpyHostToDevice, st));
-            } else {
-                NET_TRY(n, cudaMemcpyAsync(n->d_forced_stage, forced + (size_t)done * n->words, bytes, in_kind, st));
+            if (k >= 2) NET_TRY(n, cudaStreamWaitEvent(cp, n->ev_comp[b], 0));  // stage b read by chunk k-2
+            const char* src = (const char*)forced + off;
+            if (bounce_in) {
+                if (k >= 2) NET_TRY(n, cudaEventSynchronize(n->ev_in[b]));  // bounce b copied for chunk k-2
+                std::memcpy(n->h_io[b], src, bytes);
+                src = (const char*)n->h_io[b];
             }
+            NET_TRY(n, cudaMemcpyAsync(n->d_forced_stage[b], src, bytes, in_kind, cp));
+            NET_TRY(n, cudaEventRecord(n->ev_in[b], cp));
+            NET_TRY(n, cudaStreamWaitEvent(st, n->ev_in[b], 0));
         }
         if (current && n->N)
             NET_TRY(n, cudaMemcpyAsync(n->d_current_stage, current + (size_t)done * n->N, (size_t)len * n->N * 4, in_kind, st));
+        if (raster && k >= 2) NET_TRY(n, cudaStreamWaitEvent(st, n->ev_out[b], 0));  // stage b copied out
         cudaGraphExec_t ex;
-        int rc = net_graph(n, len, flags, &ex);
+        int rc = net_graph(n, len, flags, b, &ex);
         if (rc) return rc;
         NET_TRY(n, cudaGraphLaunch(ex, st));
+        NET_TRY(n, cudaEventRecord(n->ev_comp[b], st));
         n->graph_launches += 1;
-        n->kernel_launches += (uint64_t)2 * len + 1;
+        n->kernel_launches += (uint64_t)(n->overlap ? 1 : 2) * len + 1;
         if (raster) {
-            const size_t bytes = (size_t)len * n->words * 4;
-            if (host) {
-                NET_TRY(n, cudaMemcpyAsync(n->h_pinned_words, n->d_raster_stage, bytes, cudaMemcpyDeviceToHost, st));
-                NET_TRY(n, cudaStreamSynchronize(st));
-                std::memcpy(raster + (size_t)done * n->words, n->h_pinned_words, bytes);
-            } else {
-                NET_TRY(n, cudaMemcpyAsync(raster + (size_t)done * n->words, n->d_raster_stage, bytes,
-                                           cudaMemcpyDeviceToDevice, st));
-            }
+            rc = flush(b);  // bounce b last held chunk k-2
+            if (rc) return rc;
+            NET_TRY(n, cudaStreamWaitEvent(cp, n->ev_comp[b], 0));
+            char* dst = bounce_out ? (char*)n->h_io[2 + b] : (char*)raster + off;
+            NET_TRY(n, cudaMemcpyAsync(dst, n->d_raster_stage[b], bytes, out_kind, cp));
+            NET_TRY(n, cudaEventRecord(n->ev_out[b], cp));
+            if (bounce_out) pend[b] = Pending{true, off, bytes};
+            rc = flush(b ^ 1);  // chunk k-1, copied while chunk k computes
+            if (rc) return rc;
         }
         done += len;
         n->steps_done += len;
     }
+    for (int b = 0; b < 2; ++b) {
+        int rc = flush(b);
+        if (rc) return rc;
+    }
+    // the main stream resumes after the last copies
+    NET_TRY(n, cudaEventRecord(n->ev_in[0], cp));
+    NET_TRY(n, cudaStreamWaitEvent(st, n->ev_in[0], 0));
     NET_TRY(n, cudaEventRecord(n->ev_run1, st));
     n->run_timed = true;
+    if (host) NET_TRY(n, cudaStreamSynchronize(st));  // host arrays are complete on return
     return SZSNN_OK;
 }
 
@@ -1027,23 +1287,27 @@ extern "C" int szsnn_net_run_device(szsnn_net* n, int64_t steps, const uint32_t*
 
 // Per-kernel device time.  The network's state, inputs, ring counters and
 // statistics are copied to scratch buffers; a CUDA graph then replays
-// `steps` propagate launches and `steps` update launches of the current step
-// (the clock does not advance, so every replay repeats the same work:
-// propagate reads the ring slots of steps t-1..t-D and only clears slot t,
-// update re-fills slot t of the scratch counters).  Events bracket each group
-// of launches on the launching stream; the real network is left untouched.
-extern "C" int szsnn_net_profile(szsnn_net* n, int64_t steps, double* prop_ms, double* upd_ms, double* events_per_launch)
+// `steps` delivery launches, `steps` update launches and `steps` whole steps
+// of the current step (the clock does not advance, so every replay repeats the
+// same work: the delivery reads ring slots of past steps, the update re-fills
+// slot t of the scratch counters and ids of a slot that no live delivery
+// reads).  Events bracket each group of launches on the launching stream; the
+// real network is left untouched.  Overlapped order: the delivery timed alone
+// is far(t+1) (delays >= 2), the update includes its m = 1 deliveries, and the
+// whole step is the fused k_step.
+static int net_profile_impl(szsnn_net* n, int64_t steps, double* prop_ms, double* upd_ms, double* step_ms,
+                            double* events_per_launch)
 {
     if (!n || steps < 1 || steps > 100000) return SZSNN_ERR_ARG;
     cudaStream_t st = n->ctx->stream;
     const size_t U = (size_t)n->U, N = (size_t)std::max<int64_t>(n->N, 1);
     NetDev d = make_dev(n);
     float* sst[4] = {};
-    float *se = nullptr, *si = nullptr;
-    long long *sfe = nullptr, *sfi = nullptr;
+    float* sin[4] = {};        // e0, i0, e1, i1
+    long long* sfx[4] = {};
     uint32_t* scnt = nullptr;
-    unsigned long long* sstats = nullptr;
-    cudaEvent_t ev[3] = {};
+    unsigned long long* sstats = nullptr;  // [0..3] live, [4..7] copy after the delivery replays
+    cudaEvent_t ev[4] = {};
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ex = nullptr;
     cudaError_t e = cudaSuccess;
@@ -1052,47 +1316,68 @@ extern "C" int szsnn_net_profile(szsnn_net* n, int64_t steps, double* prop_ms, d
         if (g) cudaGraphDestroy(g);
         for (auto& x : ev) if (x) cudaEventDestroy(x);
         for (auto& x : sst) cudaFree(x);
-        cudaFree(se); cudaFree(si); cudaFree(sfe); cudaFree(sfi); cudaFree(scnt); cudaFree(sstats);
+        for (auto& x : sin) cudaFree(x);
+        for (auto& x : sfx) cudaFree(x);
+        cudaFree(scnt); cudaFree(sstats);
         return err;
     };
     for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
         e = dalloc(&sst[k], U);
         if (e == cudaSuccess) e = cudaMemcpyAsync(sst[k], n->d_st[k], U * 4, cudaMemcpyDeviceToDevice, st);
     }
-    if (e == cudaSuccess) e = dalloc(&se, N);
-    if (e == cudaSuccess) e = dalloc(&si, N);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(se, n->d_in_e, N * 4, cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(si, n->d_in_i, N * 4, cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess && n->acc_mode == SZSNN_ACC_FIXED) {
-        e = dalloc(&sfe, N);
-        if (e == cudaSuccess) e = dalloc(&sfi, N);
-        if (e == cudaSuccess) e = cudaMemsetAsync(sfe, 0, N * 8, st);
-        if (e == cudaSuccess) e = cudaMemsetAsync(sfi, 0, N * 8, st);
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
+        const float* src = (k & 1) ? n->d_in_i[k >> 1] : n->d_in_e[k >> 1];
+        e = dalloc(&sin[k], N);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sin[k], src, N * 4, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess && n->acc_mode == SZSNN_ACC_FIXED) {
+            e = dalloc(&sfx[k], N);
+            if (e == cudaSuccess) e = cudaMemsetAsync(sfx[k], 0, N * 8, st);
+        }
     }
     if (e == cudaSuccess) e = dalloc(&scnt, (size_t)n->R);
     if (e == cudaSuccess) e = cudaMemcpyAsync(scnt, n->d_ring_cnt, (size_t)n->R * 4, cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess) e = dalloc(&sstats, 4);
-    if (e == cudaSuccess) e = cudaMemsetAsync(sstats, 0, 32, st);
+    if (e == cudaSuccess) e = dalloc(&sstats, 8);
+    if (e == cudaSuccess) e = cudaMemsetAsync(sstats, 0, 64, st);
     for (auto& x : ev) if (e == cudaSuccess) e = cudaEventCreate(&x);
     if (e != cudaSuccess) return szsnn_set_error(n->ctx, SZSNN_ERR_CUDA, std::string("profile: ") + cudaGetErrorString(fin(e)));
     d.st0 = sst[0]; d.st1 = sst[1]; d.st2 = sst[2]; d.st3 = sst[3];
-    d.in_e = se; d.in_i = si; d.fx_e = sfe; d.fx_i = sfi;
+    d.in_e = sin[0]; d.in_i = sin[1]; d.in_e1 = sin[2]; d.in_i1 = sin[3];
+    d.fx_e = sfx[0]; d.fx_i = sfx[1]; d.fx_e1 = sfx[2]; d.fx_i1 = sfx[3];
     d.ring_cnt = scnt; d.stats = sstats; d.group = nullptr; d.group_spikes = nullptr;
     e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal);
-    for (int64_t k = 0; k < steps && e == cudaSuccess; ++k) e = launch_propagate(n, d, 0);
+    for (int64_t k = 0; k < steps && e == cudaSuccess; ++k)
+        e = n->overlap ? launch_propagate_far(n, d, 1, st) : launch_propagate_classic(n, d, 0, st);
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal);
-    for (int64_t k = 0; k < steps && e == cudaSuccess; ++k) e = launch_update(n, d, 0, nullptr, nullptr, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sstats + 4, sstats, 32, cudaMemcpyDeviceToDevice, st);
+    // each update replay re-fills slot t from empty (a replay adds the step's
+    // spikes again; without the reset a busy network would overflow the slot)
+    uint32_t* slot_t = scnt + (size_t)(n->steps_done % n->R);
+    for (int64_t k = 0; k < steps && e == cudaSuccess; ++k) {
+        e = cudaMemsetAsync(slot_t, 0, 4, st);
+        if (e == cudaSuccess) e = launch_update(n, d, 0, nullptr, nullptr, nullptr, st);
+    }
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal);
+    for (int64_t k = 0; k < steps && e == cudaSuccess; ++k) {
+        if (n->overlap) {
+            e = cudaMemsetAsync(slot_t, 0, 4, st);
+            if (e == cudaSuccess) e = launch_step(n, d, 0, nullptr, nullptr, nullptr, st);
+        } else {  // classic propagate empties slot t itself
+            e = launch_propagate_classic(n, d, 0, st);
+            if (e == cudaSuccess) e = launch_update(n, d, 0, nullptr, nullptr, nullptr, st);
+        }
+    }
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal);
     cudaError_t e2 = cudaStreamEndCapture(st, &g);
     if (e == cudaSuccess) e = e2;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
     if (e == cudaSuccess) e = cudaGraphLaunch(ex, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    float a = 0, b = 0;
-    unsigned long long hs[4] = {0, 0, 0, 0};
+    float a = 0, b = 0, c = 0;
+    unsigned long long hs[8] = {};
     if (e == cudaSuccess) e = cudaEventElapsedTime(&a, ev[0], ev[1]);
     if (e == cudaSuccess) e = cudaEventElapsedTime(&b, ev[1], ev[2]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&c, ev[2], ev[3]);
     if (e == cudaSuccess) e = cudaMemcpy(hs, sstats, sizeof(hs), cudaMemcpyDeviceToHost);
     fin(cudaSuccess);
     if (e != cudaSuccess) return szsnn_set_error(n->ctx, SZSNN_ERR_CUDA, std::string("profile: ") + cudaGetErrorString(e));
@@ -1100,8 +1385,20 @@ extern "C" int szsnn_net_profile(szsnn_net* n, int64_t steps, double* prop_ms, d
     n->t_upd_ms = b;
     if (prop_ms) *prop_ms = a;
     if (upd_ms) *upd_ms = b;
-    if (events_per_launch) *events_per_launch = (double)hs[0] / (double)steps;
+    if (step_ms) *step_ms = c;
+    if (events_per_launch) *events_per_launch = (double)(hs[4] + hs[6] + hs[7]) / (double)steps;
     return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_profile(szsnn_net* n, int64_t steps, double* prop_ms, double* upd_ms, double* events_per_launch)
+{
+    return net_profile_impl(n, steps, prop_ms, upd_ms, nullptr, events_per_launch);
+}
+
+extern "C" int szsnn_net_profile_step(szsnn_net* n, int64_t steps, double* prop_ms, double* upd_ms, double* step_ms,
+                                      double* events_per_launch)
+{
+    return net_profile_impl(n, steps, prop_ms, upd_ms, step_ms, events_per_launch);
 }
 
 extern "C" int szsnn_net_timing(szsnn_net* n, double* prop_ms, double* upd_ms, double* total_ms)
@@ -1245,7 +1542,7 @@ extern "C" int szsnn_net_restore(szsnn_net* n, const void* blob, uint64_t bytes)
     NET_TRY(n, cudaMemcpyAsync(n->d_clock, &clock, 8, cudaMemcpyHostToDevice, st));
     NET_TRY(n, cudaStreamSynchronize(st));
     n->steps_done = clock;
-    return SZSNN_OK;
+    return net_prime(n);
 }
 
 extern "C" int szsnn_net_get_synapses(szsnn_net* n, uint64_t* row_ptr, int32_t* tgt, float* w)
@@ -1422,7 +1719,7 @@ extern "C" int szsnn_step_static(const szsnn_static_step* s, char* err, size_t e
     d.clock = (const long long*)base;
     d.stats = (unsigned long long*)(base + 64);
     d.err = s->error_word ? s->error_word : (uint32_t*)(base + 128);
-    k_propagate<16><<<sms * 16, 256, 0, st>>>(d, 0);
+    k_propagate<16><<<sms * 16, 256, 0, st>>>(d, 0, 1, PF_ZERO_SLOT | PF_SPIKES);
     e = cudaGetLastError();
     if (e == cudaSuccess) {
         k_update<<<(unsigned)sz_div_up(U, 256), 256, 0, st>>>(d, 0, nullptr, nullptr, s->fired_words);

@@ -151,9 +151,17 @@ class Network:
                                         None if out is None else out.ctypes.data), self.ctx.h, "net_step")
         return out
 
-    def run(self, steps: int, forced_words=None, raster=True) -> np.ndarray | None:
+    def run(self, steps: int, forced_words=None, raster=True, out=None) -> np.ndarray | None:
+        """`steps` steps from the host: forced-spike words [steps, words] in,
+        raster words [steps, words] out.  Page-locked arrays (`out`, or
+        `forced_words`) are copied by DMA directly; pageable ones go through the
+        library's pinned bounce buffers."""
         fw = None if forced_words is None else np.ascontiguousarray(forced_words, np.uint32)
-        out = np.zeros((steps, self.words), np.uint32) if raster else None
+        if out is not None:
+            if out.dtype != np.uint32 or out.shape != (steps, self.words) or not out.flags.c_contiguous:
+                raise ValueError("out must be a C-contiguous uint32 array of shape (steps, words)")
+        elif raster:
+            out = np.zeros((steps, self.words), np.uint32)
         L.check(self.lib.szsnn_net_run(self.h, steps, None if fw is None else fw.ctypes.data,
                                        None if out is None else out.ctypes.data), self.ctx.h, "net_run")
         return out
@@ -176,8 +184,24 @@ class Network:
                 "profile")
         return p.value, u.value, ev.value
 
+    def profile_step(self, steps: int) -> dict:
+        """Device ms of `steps` replays each of the delivery launch, the update
+        launch and the whole step (overlapped: the fused launch), on scratch
+        state, and the events one delivery launch delivers."""
+        p, u, st, ev = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        L.check(self.lib.szsnn_net_profile_step(self.h, steps, C.byref(p), C.byref(u), C.byref(st), C.byref(ev)),
+                self.ctx.h, "profile_step")
+        return {"propagate_ms": p.value, "update_ms": u.value, "step_ms": st.value, "events_per_launch": ev.value}
+
     def set_tuning(self, mode: int = 0, group: int = 0, blocks: int = -1, update_block: int = 0) -> None:
         L.check(self.lib.szsnn_net_set_tuning(self.h, mode, group, blocks, update_block), self.ctx.h, "set_tuning")
+
+    overlap = True
+
+    def set_overlap(self, on: bool) -> None:
+        """Overlapped step order (default) or the classic propagate-then-update order."""
+        L.check(self.lib.szsnn_net_set_overlap(self.h, 1 if on else 0), self.ctx.h, "set_overlap")
+        self.overlap = bool(on)
 
     def stats(self) -> dict:
         s = L.NetStats()
