@@ -371,10 +371,8 @@ typedef struct {
     float* dw_in;                                   /* [M][N] out (backward) */
     float* dw_rec;                                  /* [nnz] out (backward) */
     float* dw_out;                                  /* [N][K] out (backward) */
-    const int32_t* plan_ptr;                        /* recurrent plan (szsnn_b200.pyszsnn.build_plan) or NULL: */
-    const int32_t* plan_loc;                        /*   entries grouped by (chunk of plan_chunk postsynaptic */
-    const int32_t* plan_perm;                       /*   neurons, presynaptic row); loc = target - chunk start, */
-    int32_t plan_chunk;                             /*   perm = synapse index; ptr [chunks][N+1] */
+    double* phase_ms;                               /* host [4] or NULL: backward adds its device ms per phase
+                                                       (recompute, recurrent term + dWrec, adjoint, dWin) */
     void* workspace;
     void* stream;                                   /* cudaStream_t */
 } szsnn_bptt_desc;

@@ -23,14 +23,16 @@
 //   k_bptt_spmm     R[j,b] = sum_k w_jk lam_{sign(w)}[k,b] over the CSR rows of
 //                   Wrec: the sign is folded into the column index of the
 //                   stacked [lam_e; lam_i] rows, half a warp per synapse, four
-//                   trials per lane (float4)
+//                   trials per lane (float4); the same lambda rows give the
+//                   recurrent weight gradient of that step (masked trial sum)
 //   k_bptt_adjoint  reverse-time update of (lam_u, lam_Ie, lam_Ii) per (b,i)
-//   k_bptt_dwin / k_bptt_dwrec  weight gradients, one owner per weight
+//   k_bptt_dwin     input weight gradient, one owner per weight
 #include "common.cuh"
 
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 namespace {
 
@@ -235,13 +237,32 @@ __global__ void k_bptt_colsel(const int* col, const float* val, long long nnz, i
         col_sel[q] = col[q] + (val[q] < 0.0f ? N : 0);
 }
 
-// R[j][b] = sum over row j of Wrec of w * lamS_next[col_sel][b]
-__global__ void __launch_bounds__(BP_BLOCK) k_bptt_spmm(BpttK k, const int* __restrict__ col_sel, int Bp,
-                                                        const float* __restrict__ lamS, float* __restrict__ R)
+// trials (bit b) in which input / neuron j spiked, from words [B][W] of one step
+__device__ __forceinline__ unsigned long long trial_mask(const uint32_t* words, int B, int W, int j, int lane)
 {
-    const int lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15;
+    const bool on0 = lane < B && ((words[(size_t)lane * W + (j >> 5)] >> (j & 31)) & 1u);
+    const bool on1 = lane + 32 < B && ((words[(size_t)(lane + 32) * W + (j >> 5)] >> (j & 31)) & 1u);
+    const uint32_t b0 = __ballot_sync(0xffffffffu, on0), b1 = __ballot_sync(0xffffffffu, on1);
+    return (unsigned long long)b0 | ((unsigned long long)b1 << 32);
+}
+
+// One warp per row j of Wrec, half a warp per synapse, four trials per lane:
+//   R[j][b] = sum over the row of w * lamS_next[col_sel][b]
+// and, with dw: the recurrent weight gradient of the step whose lambdas these
+// are, dWrec[e] += sum over trials b with s_step[b][j] of lamS_next[col_sel[e]][b]
+// (the same lambda row serves both; the trial sum is a fixed-order reduction
+// over the half warp).
+__global__ void __launch_bounds__(BP_BLOCK) k_bptt_spmm(BpttK k, const int* __restrict__ col_sel, int Bp,
+                                                        const float* __restrict__ lamS, float* __restrict__ R,
+                                                        float* __restrict__ dw, int s_step)
+{
+    __shared__ float s_dw[BP_BLOCK];
+    const int lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15, warp = threadIdx.x >> 5;
     const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (j >= k.N) return;
+    const unsigned long long mask =
+        dw ? trial_mask(k.spikes + (size_t)s_step * k.B * k.Nw, k.B, k.Nw, j, lane) : 0ull;
+    const uint32_t mb = (uint32_t)(mask >> (4 * hl)) & 0xFu;  // this lane's four trials
     const long long a = k.rp[j], e = k.rp[j + 1];
     const bool act = 4 * hl < Bp;
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -249,28 +270,43 @@ __global__ void __launch_bounds__(BP_BLOCK) k_bptt_spmm(BpttK k, const int* __re
         const long long kk = k0 + lane;
         const float w = kk < e ? __ldg(&k.val[kk]) : 0.0f;
         const int cs = kk < e ? __ldg(&col_sel[kk]) : 0;
+        const float dw_old = (mask && kk < e && w != 0.0f) ? dw[kk] : 0.0f;
 #pragma unroll 4
         for (int q = 0; q < 32; q += 2) {
             const float wq = __shfl_sync(0xffffffffu, w, q + half);
             const int cq = __shfl_sync(0xffffffffu, cs, q + half);
+            float part = 0.0f;
             if (act && wq != 0.0f) {
                 const float4 l = __ldg(reinterpret_cast<const float4*>(lamS + (size_t)cq * Bp) + hl);
                 acc.x += wq * l.x;
                 acc.y += wq * l.y;
                 acc.z += wq * l.z;
                 acc.w += wq * l.w;
+                part = (((mb & 1u) ? l.x : 0.0f) + ((mb & 2u) ? l.y : 0.0f)) +
+                       (((mb & 4u) ? l.z : 0.0f) + ((mb & 8u) ? l.w : 0.0f));
             }
+            if (mask) {  // warp-uniform
+                part += __shfl_xor_sync(0xffffffffu, part, 8);
+                part += __shfl_xor_sync(0xffffffffu, part, 4);
+                part += __shfl_xor_sync(0xffffffffu, part, 2);
+                part += __shfl_xor_sync(0xffffffffu, part, 1);
+                if (hl == 0) s_dw[warp * 32 + q + half] = part;
+            }
+        }
+        if (mask) {
+            __syncwarp();
+            if (kk < e && w != 0.0f) dw[kk] = dw_old + s_dw[warp * 32 + lane];
+            __syncwarp();
         }
     }
     acc.x += __shfl_down_sync(0xffffffffu, acc.x, 16);
     acc.y += __shfl_down_sync(0xffffffffu, acc.y, 16);
     acc.z += __shfl_down_sync(0xffffffffu, acc.z, 16);
     acc.w += __shfl_down_sync(0xffffffffu, acc.w, 16);
-    if (half == 0 && act) reinterpret_cast<float4*>(R + (size_t)j * Bp)[hl] = acc;
+    if (R && half == 0 && act) reinterpret_cast<float4*>(R + (size_t)j * Bp)[hl] = acc;
 }
 
-__global__ void __launch_bounds__(BP_BLOCK) k_bptt_adjoint(BpttK k, BpttBwd g, int t, int t0, int have_R,
-                                                           const float* __restrict__ part, int nchunks)
+__global__ void __launch_bounds__(BP_BLOCK) k_bptt_adjoint(BpttK k, BpttBwd g, int t, int t0, int have_R)
 {
     __shared__ float s_ly[64];
     const int b = blockIdx.y;
@@ -290,14 +326,7 @@ __global__ void __launch_bounds__(BP_BLOCK) k_bptt_adjoint(BpttK k, BpttBwd g, i
     float ro = 0.0f;
     for (int kk = 0; kk < k.K; ++kk) ro += k.w_out[(size_t)i * k.K + kk] * s_ly[kk];
     const float Gv = (g.g_vsum ? g.g_vsum[o] : 0.0f) + k.km * g.lam_u[o];
-    float rec = 0.0f;
-    if (have_R) {
-        if (part) {  // sum of the per-chunk partials, fixed order
-            for (int c = 0; c < nchunks; ++c) rec += part[((size_t)c * g.Bp + b) * k.N + i];
-        } else {
-            rec = g.R[(size_t)i * g.Bp + b];
-        }
-    }
+    const float rec = have_R ? g.R[(size_t)i * g.Bp + b] : 0.0f;
     const float Gs = ro + rec + Gv * (k.v_reset - u);
     const float lu = Gv * (s ? 0.0f : 1.0f) + Gs * surrogate(u - k.v_thresh, k.beta);
     const float le = lu / k.cm + k.de * g.lam_e[o];
@@ -313,14 +342,6 @@ __global__ void __launch_bounds__(BP_BLOCK) k_bptt_adjoint(BpttK k, BpttBwd g, i
         for (int kk = 0; kk < k.K; ++kk) atomicAdd(&g.dw_out[(size_t)i * k.K + kk], s_ly[kk]);
 }
 
-// trials (bit b) in which input / neuron j spiked, from words [B][W] of one step
-__device__ __forceinline__ unsigned long long trial_mask(const uint32_t* words, int B, int W, int j, int lane)
-{
-    const bool on0 = lane < B && ((words[(size_t)lane * W + (j >> 5)] >> (j & 31)) & 1u);
-    const bool on1 = lane + 32 < B && ((words[(size_t)(lane + 32) * W + (j >> 5)] >> (j & 31)) & 1u);
-    const uint32_t b0 = __ballot_sync(0xffffffffu, on0), b1 = __ballot_sync(0xffffffffu, on1);
-    return (unsigned long long)b0 | ((unsigned long long)b1 << 32);
-}
 
 constexpr int DWIN_J = 16;  // inputs per dwin block
 
@@ -356,142 +377,6 @@ __global__ void __launch_bounds__(BP_BLOCK) k_bptt_dwin(BpttK k, BpttBwd g, int 
     }
 }
 
-// dWrec[syn j->i] += sum over trials with s_{t-1}[b][j] of lam_{sign(w)}[i][b]
-__global__ void __launch_bounds__(BP_BLOCK) k_bptt_dwrec(BpttK k, BpttBwd g, int t)
-{
-    __shared__ unsigned long long s_mask;
-    const int j = blockIdx.x;
-    if (threadIdx.x < 32) {
-        const unsigned long long m = trial_mask(k.spikes + (size_t)(t - 1) * k.B * k.Nw, k.B, k.Nw, j, threadIdx.x);
-        if (threadIdx.x == 0) s_mask = m;
-    }
-    __syncthreads();
-    const unsigned long long mask = s_mask;
-    if (!mask) return;
-    const long long a = k.rp[j], e = k.rp[j + 1];
-    for (long long q = a + threadIdx.x; q < e; q += blockDim.x) {
-        const float w = k.val[q];
-        if (w == 0.0f) continue;
-        const float* L = g.lamS + (size_t)g.col_sel[q] * g.Bp;
-        float sum = 0.0f;
-        unsigned long long m = mask;
-        while (m) {
-            const int b = __ffsll((long long)m) - 1;
-            m &= m - 1ull;
-            sum += L[b];
-        }
-        g.dw_rec[q] += sum;
-    }
-}
-
-constexpr int REC_CT = 384;       // postsynaptic neurons per chunk of the recurrent plan
-constexpr int REC_THREADS = 512;
-
-struct RecPlan {
-    const int* ptr;       // [nchunks][N+1]: entries of (chunk, presynaptic row)
-    const int* loc;       // [nnz] postsynaptic neuron - chunk start
-    const float* val;     // [nnz] weights in plan order
-    float* dw;            // [nnz] weight gradient in plan order
-    const unsigned long long* mask;  // [N] trials in which each neuron spiked at step t-1
-    float* part;          // [nchunks][Bp][N] recurrent-term partials for step t-1
-    int nchunks;
-};
-
-// trials in which neuron j spiked at step s (bit b)
-__global__ void k_bptt_masks(BpttK k, int s, unsigned long long* mask)
-{
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= k.N) return;
-    const uint32_t* w = k.spikes + (size_t)s * k.B * k.Nw + (j >> 5);
-    unsigned long long m = 0;
-    for (int b = 0; b < k.B; ++b) m |= (unsigned long long)((w[(size_t)b * k.Nw] >> (j & 31)) & 1u) << b;
-    mask[j] = m;
-}
-
-// Step t of the reverse sweep for the recurrent weights, one CTA per (target
-// chunk, row split): with lam_t of the chunk's neurons staged in shared memory,
-//   dw[e]         += sum over trials b spiking at t-1 in row j of lam_t[sign(w)][tgt][b]
-//   part[c][b][j]  = sum over the row's entries in chunk c of w * lam_t[sign(w)][tgt][b]
-// (part summed over chunks is the recurrent term of step t-1).
-__global__ void __launch_bounds__(REC_THREADS) k_bptt_rec(BpttK k, RecPlan r, const float* __restrict__ lamS, int Bp)
-{
-    extern __shared__ float s_mem[];
-    const int Bs = Bp + 1;                 // odd row stride: conflict-free column reads
-    float* s_lam = s_mem;                  // [2][REC_CT][Bs]
-    float* s_tile = s_mem + 2 * REC_CT * Bs;  // [32][Bs]
-    const int c = blockIdx.x;
-    const int t0c = c * REC_CT;
-    const int nt = min(REC_CT, k.N - t0c);
-    for (int idx = threadIdx.x; idx < 2 * nt * Bp; idx += blockDim.x) {
-        const int h = idx / (nt * Bp), rem = idx - h * nt * Bp, q = rem / Bp, b = rem - q * Bp;
-        s_lam[(h * REC_CT + q) * Bs + b] = lamS[((size_t)h * k.N + t0c + q) * Bp + b];
-    }
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int per = (k.N + gridDim.y - 1) / gridDim.y;
-    const int r0 = blockIdx.y * per, r1 = min(k.N, r0 + per);
-    const int* ptr = r.ptr + (size_t)c * (k.N + 1);
-    for (int jt = r0; jt < r1; jt += 32) {
-        for (int jj = warp; jj < 32; jj += nwarps) {
-            const int j = jt + jj;
-            float acc0 = 0.0f, acc1 = 0.0f;
-            if (j < r1) {
-                const int e0 = ptr[j], e1 = ptr[j + 1];
-                const unsigned long long mask = r.mask[j];
-                for (int eb = e0; eb < e1; eb += 32) {
-                    const int e = eb + lane;
-                    const bool valid = e < e1;
-                    const float w = valid ? r.val[e] : 0.0f;
-                    const int loc = valid ? r.loc[e] : 0;
-                    if (valid && mask && w != 0.0f) {
-                        const float* sel = s_lam + ((w >= 0.0f ? 0 : REC_CT) + loc) * Bs;
-                        float sum = 0.0f;
-                        unsigned long long m = mask;
-                        while (m) {
-                            const int b = __ffsll((long long)m) - 1;
-                            m &= m - 1ull;
-                            sum += sel[b];
-                        }
-                        r.dw[e] += sum;
-                    }
-                    const int n = min(32, e1 - eb);
-                    for (int q = 0; q < n; ++q) {
-                        const float wq = __shfl_sync(0xffffffffu, w, q);
-                        const int lq = __shfl_sync(0xffffffffu, loc, q);
-                        if (wq != 0.0f) {
-                            const float* sel = s_lam + ((wq >= 0.0f ? 0 : REC_CT) + lq) * Bs;
-                            if (lane < Bp) acc0 = __fmaf_rn(wq, sel[lane], acc0);
-                            if (lane + 32 < Bp) acc1 = __fmaf_rn(wq, sel[lane + 32], acc1);
-                        }
-                    }
-                }
-            }
-            if (lane < Bp) s_tile[jj * Bs + lane] = acc0;
-            if (lane + 32 < Bp) s_tile[jj * Bs + lane + 32] = acc1;
-        }
-        __syncthreads();
-        if (r.part) {
-            for (int idx = threadIdx.x; idx < Bp * 32; idx += blockDim.x) {
-                const int b = idx >> 5, jj = idx & 31, j = jt + jj;
-                if (j < r1) r.part[((size_t)c * Bp + b) * k.N + j] = s_tile[jj * Bs + b];
-            }
-        }
-        __syncthreads();
-    }
-}
-
-__global__ void k_bptt_gather_val(const int* perm, const float* val, long long nnz, float* out)
-{
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x)
-        out[e] = val[perm[e]];
-}
-
-__global__ void k_bptt_scatter_dw(const int* perm, const float* dw_plan, long long nnz, float* dw)
-{
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x)
-        dw[perm[e]] = dw_plan[e];
-}
-
 __global__ void k_bptt_fill_dense(const long long* rp, const int* col, const float* val, int N, float* dense)
 {
     const int j = blockIdx.x;
@@ -507,8 +392,7 @@ __global__ void k_bptt_init(float* ymax, int* tmax, int n)
 }
 
 struct Work {
-    size_t dense, Ie, Ii, v, y, u_seg, lam_u, lam_e, lam_i, lamS0, lamS1, lamT, R, ly0, ly1, colsel, pval, pdw, pmask,
-        part, total;
+    size_t dense, Ie, Ii, v, y, u_seg, lam_u, lam_e, lam_i, lamS0, lamS1, lamT, R, ly0, ly1, colsel, total;
 };
 
 int bp_pad(int B) { return (B + 3) / 4 * 4; }
@@ -526,13 +410,6 @@ Work layout(const szsnn_bptt_desc* d)
     w.lamS0 = take(2 * NBp); w.lamS1 = take(2 * NBp); w.lamT = take(2 * BN);
     w.R = take(NBp); w.ly0 = take(BK); w.ly1 = take(BK);
     w.colsel = take((size_t)d->nnz);  // ints, same size as floats
-    if (d->plan_ptr) {
-        const size_t nchunks = (size_t)(d->N + REC_CT - 1) / REC_CT;
-        w.pval = take((size_t)d->nnz);
-        w.pdw = take((size_t)d->nnz);
-        w.pmask = take((size_t)d->N * 2);  // uint64
-        w.part = take(nchunks * bp_pad(d->B) * (size_t)d->N);
-    }
     w.total = o * sizeof(float);
     return w;
 }
@@ -550,8 +427,6 @@ int check_desc(const szsnn_bptt_desc* d, char* err, size_t len)
     if (d->tau_refrac != 0.0f) return fail("the adjoint supports tau_refrac == 0 only");
     if ((size_t)(d->M + d->N) * 4 > 200 * 1024) return fail("inputs + neurons exceed the shared-memory spike lists");
     if (d->N % 4) return fail("neurons must be a multiple of 4");
-    if (d->plan_ptr && (!d->plan_loc || !d->plan_perm || d->plan_chunk != REC_CT))
-        return fail("recurrent plan incomplete or built for another chunk size");
     return SZSNN_OK;
 }
 
@@ -583,6 +458,40 @@ size_t step_smem(const szsnn_bptt_desc* d) { return (size_t)(d->M + d->N) * size
             return SZSNN_ERR_CUDA;                                                             \
         }                                                                                      \
     } while (0)
+
+// Device time per phase, from CUDA events recorded on the stream between
+// launches (only when the caller asks for it: it adds a synchronisation at the end).
+struct PhaseTimer {
+    double* out;
+    cudaStream_t st;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> phase;
+    PhaseTimer(double* o, cudaStream_t s) : out(o), st(s) {}
+    ~PhaseTimer() { for (cudaEvent_t e : ev) cudaEventDestroy(e); }
+    void mark(int ph)  // end of phase `ph` (-1: a start point)
+    {
+        if (!out) return;
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) { out = nullptr; return; }
+        cudaEventRecord(e, st);
+        ev.push_back(e);
+        phase.push_back(ph);
+    }
+    cudaError_t finish()
+    {
+        if (!out || ev.empty()) return cudaSuccess;
+        cudaError_t e = cudaEventSynchronize(ev.back());
+        if (e != cudaSuccess) return e;
+        for (size_t i = 1; i < ev.size(); ++i) {
+            if (phase[i] < 0) continue;
+            float ms = 0.0f;
+            e = cudaEventElapsedTime(&ms, ev[i - 1], ev[i]);
+            if (e != cudaSuccess) return e;
+            out[phase[i]] += ms;
+        }
+        return cudaSuccess;
+    }
+};
 
 extern "C" int szsnn_bptt_workspace_bytes(const szsnn_bptt_desc* d, uint64_t* bytes)
 {
@@ -654,33 +563,17 @@ extern "C" int szsnn_bptt_backward(const szsnn_bptt_desc* d, char* err, size_t e
     BP_TRY(cudaMemsetAsync(d->dw_in, 0, (size_t)d->M * d->N * 4, st));
     BP_TRY(cudaMemsetAsync(d->dw_rec, 0, (size_t)d->nnz * 4, st));
     BP_TRY(cudaMemsetAsync(d->dw_out, 0, (size_t)d->N * d->K * 4, st));
-    const bool plan = d->plan_ptr != nullptr;
-    RecPlan rp{};
-    rp.nchunks = (d->N + REC_CT - 1) / REC_CT;
-    const int rec_split = std::max(1, (148 + rp.nchunks - 1) / rp.nchunks);
-    const size_t rec_smem = (size_t)(2 * REC_CT + 32) * (Bp + 1) * sizeof(float);
-    if (plan) {
-        rp.ptr = d->plan_ptr;
-        rp.loc = d->plan_loc;
-        rp.val = ws + w.pval;
-        rp.dw = ws + w.pdw;
-        rp.mask = reinterpret_cast<const unsigned long long*>(ws + w.pmask);
-        rp.part = ws + w.part;
-        BP_TRY(cudaMemsetAsync(ws + w.pdw, 0, (size_t)d->nnz * 4, st));
-        if (d->nnz > 0) {
-            k_bptt_gather_val<<<1024, 256, 0, st>>>(d->plan_perm, k.val, d->nnz, ws + w.pval);
-            BP_TRY(cudaGetLastError());
-        }
-        BP_TRY(cudaFuncSetAttribute(k_bptt_rec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rec_smem));
-    } else if (d->nnz > 0) {
+    if (d->nnz > 0) {
         k_bptt_colsel<<<1024, 256, 0, st>>>(k.col, k.val, d->nnz, d->N, col_sel);
         BP_TRY(cudaGetLastError());
     }
+    const unsigned spmm_blocks = (unsigned)sz_div_up((int64_t)d->N * 32, BP_BLOCK);
+    // optional per-phase device time (recompute, recurrent term + dWrec, adjoint, dWin)
+    PhaseTimer pt(d->phase_ms, st);
     const size_t smem = step_smem(d);
     const dim3 grid_step((unsigned)sz_div_up(d->N, BP_BLOCK * BP_NPT), (unsigned)d->B);
     const dim3 grid((unsigned)sz_div_up(d->N, BP_BLOCK), (unsigned)d->B);
     const dim3 grid_in((unsigned)sz_div_up(d->N, BP_BLOCK), (unsigned)sz_div_up(d->M, DWIN_J));
-    const unsigned spmm_blocks = (unsigned)sz_div_up((int64_t)d->N * 32, BP_BLOCK);
     const int nseg = (d->T + d->checkpoint_every - 1) / d->checkpoint_every;
     for (int seg = nseg - 1; seg >= 0; --seg) {
         const int t0 = seg * d->checkpoint_every, t1 = std::min(d->T, t0 + d->checkpoint_every);
@@ -688,42 +581,31 @@ extern "C" int szsnn_bptt_backward(const szsnn_bptt_desc* d, char* err, size_t e
         BP_TRY(cudaMemcpyAsync(k.Ie, c, BN * 4, cudaMemcpyDeviceToDevice, st));
         BP_TRY(cudaMemcpyAsync(k.Ii, c + BN, BN * 4, cudaMemcpyDeviceToDevice, st));
         BP_TRY(cudaMemcpyAsync(k.v, c + 2 * BN, BN * 4, cudaMemcpyDeviceToDevice, st));
+        pt.mark(-1);
         for (int t = t0; t < t1; ++t) {  // recompute u_t from the checkpoint, spikes kept
             k_bptt_step<<<grid_step, BP_BLOCK, smem, st>>>(k, t, 1, t0);
             BP_TRY(cudaGetLastError());
         }
+        pt.mark(0);
         for (int t = t1 - 1; t >= t0; --t) {
             const int par = t & 1;  // buffers of step t; step t+1 uses the other parity
             const bool have_R = t < d->T - 1;
-            if (have_R && !plan) {
-                k_bptt_spmm<<<spmm_blocks, BP_BLOCK, 0, st>>>(k, col_sel, Bp, lamS[par ^ 1], ws + w.R);
+            if (have_R) {  // R from lambda_{t+1}, and dWrec of step t+1 (spikes of step t)
+                k_bptt_spmm<<<spmm_blocks, BP_BLOCK, 0, st>>>(k, col_sel, Bp, lamS[par ^ 1], ws + w.R, d->dw_rec, t);
                 BP_TRY(cudaGetLastError());
             }
+            pt.mark(1);
             g.lamS = lamS[par];
             g.lam_y = lamY[par];
             g.lam_y_next = lamY[par ^ 1];
-            k_bptt_adjoint<<<grid, BP_BLOCK, 0, st>>>(k, g, t, t0, have_R ? 1 : 0, plan ? rp.part : nullptr,
-                                                     rp.nchunks);
+            k_bptt_adjoint<<<grid, BP_BLOCK, 0, st>>>(k, g, t, t0, have_R ? 1 : 0);
             BP_TRY(cudaGetLastError());
+            pt.mark(2);
             k_bptt_dwin<<<grid_in, BP_BLOCK, 0, st>>>(k, g, t);
             BP_TRY(cudaGetLastError());
-            if (t >= 1) {
-                if (plan) {
-                    k_bptt_masks<<<(unsigned)sz_div_up(d->N, 256), 256, 0, st>>>(k, t - 1, (unsigned long long*)rp.mask);
-                    BP_TRY(cudaGetLastError());
-                    k_bptt_rec<<<dim3((unsigned)rp.nchunks, (unsigned)rec_split), REC_THREADS, rec_smem, st>>>(
-                        k, rp, lamS[par], Bp);
-                    BP_TRY(cudaGetLastError());
-                } else {
-                    k_bptt_dwrec<<<d->N, BP_BLOCK, 0, st>>>(k, g, t);
-                    BP_TRY(cudaGetLastError());
-                }
-            }
+            pt.mark(3);
         }
     }
-    if (plan && d->nnz > 0) {
-        k_bptt_scatter_dw<<<1024, 256, 0, st>>>(d->plan_perm, rp.dw, d->nnz, d->dw_rec);
-        BP_TRY(cudaGetLastError());
-    }
+    BP_TRY(pt.finish());
     return SZSNN_OK;
 }

@@ -37,11 +37,10 @@ class BpttDesc(C.Structure):
                 ("w_out", C.c_void_p), ("x_bits", C.c_void_p), ("v0", C.c_void_p), ("spikes", C.c_void_p),
                 ("ckpt", C.c_void_p), ("ymax", C.c_void_p), ("tmax", C.c_void_p), ("vsum", C.c_void_p),
                 ("u_trace", C.c_void_p), ("g_ymax", C.c_void_p), ("g_vsum", C.c_void_p), ("dw_in", C.c_void_p), ("dw_rec", C.c_void_p),
-                ("dw_out", C.c_void_p), ("plan_ptr", C.c_void_p), ("plan_loc", C.c_void_p),
-                ("plan_perm", C.c_void_p), ("plan_chunk", C.c_int32), ("workspace", C.c_void_p),
+                ("dw_out", C.c_void_p), ("phase_ms", C.c_void_p), ("workspace", C.c_void_p),
                 ("stream", C.c_void_p)]
 
-PLAN_CHUNK = 384  # postsynaptic neurons per chunk of the recurrent plan (the kernel's compile-time tile)
+BACKWARD_PHASES = ("recompute", "recurrent term + dWrec", "adjoint", "dWin")
 
 
 @dataclass
@@ -58,23 +57,12 @@ class LIFCurrExpRNN:
     alpha: float = 0.95
     beta: float = 10.0
     checkpoint_every: int = 50
-    use_plan: bool = False             # fused chunked recurrent backward (else per-row SpMM + dW kernels)
-    _plan: tuple | None = field(default=None, repr=False)
+    phase_ms: np.ndarray | None = field(default=None, repr=False)  # float64 [4]: backward adds its device ms
+                                                                    # per phase (BACKWARD_PHASES) when set
 
     @property
     def nnz(self) -> int:
         return int(self.rec_col.numel())
-
-    def plan(self) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor] | None:
-        """Recurrent plan for the backward, built once from the fixed CSR
-        structure: synapses grouped by (chunk of PLAN_CHUNK postsynaptic
-        neurons, presynaptic row), in CSR order inside a group.
-        Returns (ptr int32 [chunks][N+1], loc int32 [nnz], perm int32 [nnz])."""
-        if not self.use_plan:
-            return None
-        if self._plan is None:
-            self._plan = build_plan(self.rec_row_ptr, self.rec_col, self.n_neurons)
-        return self._plan
 
 
 def _ptr(t):
@@ -91,10 +79,6 @@ def _desc(net: LIFCurrExpRNN, B: int, T: int, tensors: dict) -> BpttDesc:
     d.v_reset, d.v_thresh = p["v_reset"], p["v_thresh"]
     d.alpha, d.beta, d.nnz = net.alpha, net.beta, net.nnz
     d.rec_row_ptr, d.rec_col = _ptr(net.rec_row_ptr), _ptr(net.rec_col)
-    plan = net.plan()
-    if plan is not None:
-        d.plan_ptr, d.plan_loc, d.plan_perm = (_ptr(t) for t in plan)
-        d.plan_chunk = PLAN_CHUNK
     for k, v in tensors.items():
         setattr(d, k, _ptr(v))
     d.stream = torch.cuda.current_stream().cuda_stream
@@ -155,32 +139,13 @@ class LIFCurrExpFunction(torch.autograd.Function):
         d = _desc(net, B, T, dict(w_in=w_in, rec_val=rec_val, w_out=w_out, x_bits=x_bits, v0=v0, spikes=spikes,
                                   ckpt=ckpt, tmax=tmax, g_ymax=g_ymax, g_vsum=g_vsum, dw_in=dw_in, dw_rec=dw_rec,
                                   dw_out=dw_out, workspace=ctx.ws))
+        if net.phase_ms is not None:
+            if net.phase_ms.dtype != np.float64 or net.phase_ms.shape != (4,) or not net.phase_ms.flags.c_contiguous:
+                raise ValueError("phase_ms must be a contiguous float64 array of 4")
+            d.phase_ms = net.phase_ms.ctypes.data
         msg = C.create_string_buffer(256)
         _check(L.lib().szsnn_bptt_backward(C.byref(d), msg, 256), msg)
         return dw_in, dw_rec, dw_out, None, None, None
-
-
-def build_plan(row_ptr: torch.Tensor, col: torch.Tensor, n: int, chunk: int = PLAN_CHUNK):
-    """(ptr [chunks][n+1], loc, perm) int32 device tensors: synapse perm[e] is
-    entry e of the plan, entries of (chunk c, row j) are ptr[c][j] ..
-    ptr[c][j+1]-1, loc = postsynaptic neuron - c * chunk."""
-    rp = row_ptr.cpu().numpy().astype(np.int64)
-    cl = col.cpu().numpy().astype(np.int64)
-    nnz = cl.size
-    if nnz >= 2 ** 31:
-        raise ValueError("recurrent plan: more than 2^31 - 1 synapses")
-    nch = (n + chunk - 1) // chunk
-    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(rp))
-    key = (cl // chunk) * n + rows
-    perm = np.argsort(key, kind="stable")
-    off = np.zeros(nch * n + 1, np.int64)
-    np.cumsum(np.bincount(key, minlength=nch * n), out=off[1:])
-    ptr = np.empty((nch, n + 1), np.int64)
-    ptr[:, :n] = off[:-1].reshape(nch, n)
-    ptr[:, n] = off[n::n]
-    loc = cl[perm] - (cl[perm] // chunk) * chunk
-    dev = col.device
-    return tuple(torch.from_numpy(a.astype(np.int32)).to(dev) for a in (ptr, loc, perm))
 
 
 def simulate(net: LIFCurrExpRNN, w_in, rec_val, w_out, x_bits, v0, trace_u: bool = False) -> dict:
