@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="keep the default launch shape instead of autotuning after the warm-up")
     ap.add_argument("--tune-after", type=int, default=3000, help="steps simulated before the tuner's replays")
+    ap.add_argument("--shape", default=None,
+                    help="fixed launch shape 'order,mode,group,blocks,update_block' (order: overlapped|classic) "
+                         "instead of the tuner")
     ap.add_argument("--e2e-steps", type=int, default=1000)
     ap.add_argument("--profile-steps", type=int, default=200)
     ap.add_argument("--cpu-neurons", type=int, default=50_000)
@@ -338,7 +341,15 @@ def main():
     net.run_device(args.warmup)
     ctx.sync()
     tuning = None
-    if args.tune:  # past the start-up transient (v(0) ~ U(-60,-50) fires a first volley)
+    if args.shape:
+        order, mode, group, blocks_, ub = args.shape.split(",")
+        net.set_overlap(order == "overlapped")
+        net.set_tuning(int(mode), int(group), int(blocks_), int(ub))
+        tuning = {"overlap": order == "overlapped", "mode": int(mode), "group": int(group), "blocks": int(blocks_),
+                  "update_block": int(ub), "source": "--shape"}
+        net.run_device(args.warmup)
+        ctx.sync()
+    elif args.tune:  # past the start-up transient (v(0) ~ U(-60,-50) fires a first volley)
         from szsnn_b200.autotune import tune
         net.run_device(max(0, args.tune_after - args.warmup))
         ctx.sync()

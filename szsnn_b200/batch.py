@@ -213,3 +213,50 @@ def compare_batched_looped(ctx, specs: list[NetSpec], steps: int = 1000, acc_mod
                 neurons=int(sum(s.n for s in specs)),
                 synapses=int(batch.net.n_synapses), spikes_batched=s_batch, spikes_looped=s_loop,
                 events_batched=int(st["events"]))
+
+
+def _main(argv=None) -> None:
+    """Run a batched sweep from the command line:
+    python -m szsnn_b200.batch [--nets N] [--every K] [--steps S] [--warmup W]
+                               [--shape order,mode,group,blocks,update_block | --tune]
+    --every K keeps every K-th net of the 512-net sweep (a smaller batch of the same mix)."""
+    import argparse
+    import json
+
+    from .context import Context
+
+    ap = argparse.ArgumentParser(prog="python -m szsnn_b200.batch")
+    ap.add_argument("--nets", type=int, default=512)
+    ap.add_argument("--every", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=300)
+    ap.add_argument("--shape", default=None)
+    ap.add_argument("--tune", action="store_true")
+    a = ap.parse_args(argv)
+    ctx = Context(0)
+    specs = sweep_specs(a.nets, seed=0)[:: a.every]
+    bt = Batch(ctx, specs)
+    if a.shape:
+        order, mode, group, blocks, ub = a.shape.split(",")
+        bt.net.set_overlap(order == "overlapped")
+        bt.net.set_tuning(int(mode), int(group), int(blocks), int(ub))
+    bt.run(a.warmup)
+    ctx.sync()
+    choice = None
+    if a.tune:
+        from .autotune import tune as _tune
+        choice = {k: v for k, v in _tune(bt.net).items() if k != "trials"}
+    s0 = bt.net.stats()
+    bt.run(a.steps)
+    ctx.sync()
+    s1 = bt.net.stats()
+    ms = bt.net.device_ms()
+    print(json.dumps({"nets": len(specs), "units": bt.net.U, "synapses": bt.net.n_synapses, "steps": a.steps,
+                      "device_ms": ms, "events_per_step": (s1["events"] - s0["events"]) / max(a.steps, 1),
+                      "nets_per_s": len(specs) / (ms / 1e3), "tuning": choice}))
+    bt.close()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    _main()

@@ -53,7 +53,6 @@ struct NetDev {
     const PopDev* pops;
     const unsigned long long* row_ptr;
     const int2* syn;
-    unsigned long long n_syn;  // synapses in syn[] (bounds the L2 prefetches; 0 disables them)
     float* st0;
     float* st1;
     float* st2;
@@ -189,24 +188,6 @@ __device__ __forceinline__ void deliver(const NetDev& nd, const InBuf& b, int2 s
     }
 }
 
-// Bucket [a, e) of syn[] into L2 ahead of its use (the next step reads the
-// bucket after the one this step reads: a spike's delay buckets are
-// contiguous).  One bulk prefetch per bucket, 16-byte aligned, kept inside the
-// array's first n_syn entries.
-__device__ __forceinline__ void l2_prefetch_bucket(const NetDev& nd, unsigned long long a, unsigned long long e)
-{
-    if (e > nd.n_syn) e = nd.n_syn;
-    if (e <= a) return;
-    const uintptr_t base = (uintptr_t)nd.syn;
-    const uintptr_t lo = (base + a * 8) & ~(uintptr_t)15;
-    uintptr_t hi = (base + e * 8 + 15) & ~(uintptr_t)15;
-    const uintptr_t lim = (base + nd.n_syn * 8) & ~(uintptr_t)15;
-    if (hi > lim) hi = lim;
-    if (hi <= lo) return;
-    const uint32_t bytes = (uint32_t)min((uintptr_t)(hi - lo), (uintptr_t)(1u << 16));
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"(bytes) : "memory");
-}
-
 // ring-slot counts of delays m_lo..D for step t, inclusive scan in s_pre[1..D]
 // (s_pre[0] = 0); block 0 does the slot / statistics bookkeeping of `pf`
 __device__ __forceinline__ void propagate_prologue(const NetDev& nd, long long t, int m_lo, uint32_t pf,
@@ -282,7 +263,6 @@ __device__ __forceinline__ void propagate_grouped(const NetDev& nd, int k_off, i
         const int64_t s = nd.ring_ids[slot * nd.U + j];
         const unsigned long long a = nd.row_ptr[s * D + (m - 1)];
         const unsigned long long e = nd.row_ptr[s * D + m];
-        if (lg == 0 && m < D) l2_prefetch_bucket(nd, e, nd.row_ptr[s * D + m + 1]);  // bucket m+1: next step
         for (unsigned long long q = a + lg; q < e; q += G) deliver(nd, buf, nd.syn[q], ev);
     }
     propagate_epilogue(nd, t, pf, ev, &s_ev);
@@ -329,7 +309,6 @@ __device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int 
             const int64_t s = __ldg(&nd.ring_ids[((t - m) % R) * nd.U + j]);
             a = __ldg(&nd.row_ptr[s * D + (m - 1)]);
             e = __ldg(&nd.row_ptr[s * D + m]);
-            if (m < D) l2_prefetch_bucket(nd, e, __ldg(&nd.row_ptr[s * D + m + 1]));  // bucket m+1: next step
         }
         const uint32_t len = (uint32_t)(e - a);
         uint32_t incl = len;
@@ -508,7 +487,6 @@ __device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk
             if (spk) {
                 ra = nd.row_ptr[id * nd.D];
                 re = nd.row_ptr[id * nd.D + 1];
-                if (nd.D >= 2) l2_prefetch_bucket(nd, re, nd.row_ptr[id * nd.D + 2]);  // bucket 2: step t+2
             }
             uint32_t ev = 0;
             for (uint32_t bits = ball; bits; bits &= bits - 1u) {
@@ -665,7 +643,7 @@ NetDev make_dev(szsnn_net* n)
 {
     NetDev d{};
     d.N = n->N; d.U = n->U; d.words = n->words; d.D = n->D; d.npops = n->npops;
-    d.pops = n->d_pops; d.row_ptr = n->d_row_ptr; d.syn = n->d_syn; d.n_syn = n->n_syn;
+    d.pops = n->d_pops; d.row_ptr = n->d_row_ptr; d.syn = n->d_syn;
     d.st0 = n->d_st[0]; d.st1 = n->d_st[1]; d.st2 = n->d_st[2]; d.st3 = n->d_st[3];
     d.in_e = n->d_in_e[0]; d.in_i = n->d_in_i[0]; d.fx_e = n->d_fx_e[0]; d.fx_i = n->d_fx_i[0];
     d.in_e1 = n->d_in_e[1]; d.in_i1 = n->d_in_i[1]; d.fx_e1 = n->d_fx_e[1]; d.fx_i1 = n->d_fx_i[1];
