@@ -45,7 +45,10 @@ BYTES_PER_NEURON = 48    # 16 B state read + 16 B write + 8 B input read + 8 B c
 # neurons x 1000 synapses (152,640 events per launch), scaled by events.
 NCU_UPDATE_TRAFFIC = 24_420_352
 NCU_PROPAGATE_TRAFFIC_PER_EVENT = 5_706_752 / 152_640
-NCU_STEP_TRAFFIC = None  # k_step at 1.1M units: not captured yet
+# k_step at 1.1M units and fan-out 100 (245,471 events per launch): 72.5 MB; the per-(spike, delay)
+# item traffic is the same at fan-out 1000, each further event adds its 8 B synapse
+NCU_STEP_TRAFFIC_FANOUT100 = 72_515_328
+NCU_STEP_EVENTS_FANOUT100 = 245_471
 
 
 def parse():
@@ -414,7 +417,9 @@ def main():
         # delay-1 buckets of its spikes and the delay >= 2 delivery of the next step
         step_bytes = upd_bytes + ev_step * BYTES_PER_EVENT
         dom = {"kernel": "k_step", "achieved": step_bytes / (step_us * 1e-6) / 1e9, "bytes_per_launch": step_bytes,
-               "us_per_launch": step_us, "traffic": NCU_STEP_TRAFFIC if n + p == 1_100_000 else None}
+               "us_per_launch": step_us,
+               "traffic": int(NCU_STEP_TRAFFIC_FANOUT100 + max(0.0, ev_step - NCU_STEP_EVENTS_FANOUT100) * 8)
+               if n + p == 1_100_000 else None}
     elif prop_us >= upd_us:
         dom = {"kernel": "k_propagate", "achieved": prop_bytes / (prop_us * 1e-6) / 1e9,
                "bytes_per_launch": prop_bytes, "us_per_launch": prop_us,
