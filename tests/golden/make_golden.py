@@ -13,6 +13,9 @@ Sources (paths inside the reference project):
       IF_curr_exp run: for neuron 1 of partition 0 the kernel prints, each
       cycle, Ie / Ii with their input sums and V with last value, rest, tau,
       reset, I, cm and delta (IF_curr_exp_update_kernel.cl:241-242,267-269).
+  szsnn1.1/bin/izi1.conn~, izi2.conn~   the connection files of the reference's
+      100-neuron Izhikevich example (src/main.cpp:139-142): 80 excitatory and
+      20 inhibitory sources; copied byte for byte as izi1.conn / izi2.conn.
 """
 from __future__ import annotations
 
@@ -70,7 +73,12 @@ def main(ref: str) -> None:
     np.savez_compressed(os.path.join(HERE, "pynn_2neuron_v.npz"), v=tr)
     lg = szsnn_log(ref)
     np.savez_compressed(os.path.join(HERE, "szsnn_if_curr_exp_log.npz"), **lg)
-    print(f"pynn trace: {len(tr)} steps; szsnn log: {len(lg['v'])} cycles")
+    for name in ("izi1", "izi2"):
+        with open(os.path.join(ref, "szsnn1.1", "bin", name + ".conn~"), "rb") as f:
+            data = f.read()
+        with open(os.path.join(HERE, name + ".conn"), "wb") as f:
+            f.write(data)
+    print(f"pynn trace: {len(tr)} steps; szsnn log: {len(lg['v'])} cycles; izi1/izi2.conn copied")
 
 
 if __name__ == "__main__":

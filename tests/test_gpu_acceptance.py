@@ -1,0 +1,203 @@
+"""GPU: the acceptance bar per configuration, fp32 atomic accumulation (the
+default) against the oracle on the same connectivity, delays and input spikes.
+
+For each workload:
+  * spike rasters bit-exact for the first 100 steps;
+  * membrane and synaptic state within 1e-5 relative until the first threshold
+    flip (the last state snapshot before the first step whose raster differs,
+    or the end of the run when none does);
+  * population rate and ISI-CV (pooled inter-spike intervals of the neurons)
+    within 1 % over the full run;
+  * against the oracle's FP64 twin (same equations in double): rasters equal
+    for at least the first 50 steps, the membrane within 1e-4 relative at step
+    50 and within 1e-2 at the last snapshot before the first flip (chaotic
+    dynamics amplify the fp32 rounding from there); the measured figures are
+    printed for the record.
+
+Workloads:
+  1. Izhikevich pulse-coupled network, 1000 neurons (800 RS / 200 FS), 100
+     targets each, weights 6 / -5, excitatory delays U{1..20}, thalamic input,
+     1000 single 1 ms steps;
+  2. IF_curr_exp balanced network, 3200 / 800 neurons, connection probability
+     0.02, w 0.25 / -2.25 nA, delays U{1..100} steps at dt 0.1 ms, 1000 Poisson
+     sources at 10 Hz with fan-out probability 0.02, 10,000 steps;
+  3. the 1M IF_cond_exp benchmark network (bench.cond_config: fan-out 1000,
+     delays U{1..64}, 10 % Poisson sources at 5 Hz) at 100k neurons so the
+     oracle finishes in seconds, 2000 steps.
+Workloads 1 and 2 have dyadic weights, so every fp32 sum is exact whatever the
+atomic order: the whole run is bit-exact.  Workload 3's continuous weights make
+the order matter, so its trajectory may depart from the oracle's after a first
+flip; the statistics then carry the comparison.
+"""
+import json
+
+import numpy as np
+import pytest
+
+import oracle
+import szsnn_b200 as sz
+from tests.helpers import izh_network, thalamic
+
+pytestmark = pytest.mark.gpu
+
+SNAP = 50  # state snapshots every SNAP steps
+
+
+@pytest.fixture(scope="module")
+def ctx(built):
+    c = sz.Context(0)
+    yield c
+    c.close()
+
+
+def _bits(raster, n):
+    return np.unpackbits(raster.view(np.uint8), bitorder="little").reshape(raster.shape[0], -1)[:, :n].astype(bool)
+
+
+def _rate_cv(raster, n, dt_ms):
+    b = _bits(raster, n)
+    steps = b.shape[0]
+    rate = b.sum() / n / (steps * dt_ms * 1e-3)
+    t, i = np.nonzero(b)
+    order = np.lexsort((t, i))
+    t, i = t[order], i[order]
+    same = i[1:] == i[:-1]
+    isi = (t[1:] - t[:-1])[same].astype(np.float64)
+    cv = isi.std() / isi.mean() if isi.size > 10 else float("nan")
+    return rate, cv, int(b.sum())
+
+
+def _run_snapshots(run, steps, get_state):
+    """run(k) -> raster [k][W]; returns the raster and the state every SNAP steps."""
+    parts, snaps = [], {}
+    done = 0
+    while done < steps:
+        k = min(SNAP, steps - done)
+        parts.append(run(k))
+        done += k
+        snaps[done] = [s.copy() for s in get_state()]
+    return np.concatenate(parts), snaps
+
+
+def _check(name, net, onet, o64, n, steps, dt_ms, cur=None):
+    W = net.words
+
+    def gpu_run(k):
+        if cur is None:
+            return net.run(k)
+        t0 = gpu_run.t
+        gpu_run.t += k
+        return np.stack([net.step(current=cur[t]) for t in range(t0, t0 + k)])
+    gpu_run.t = 0
+
+    def orc(o):
+        def f(k):
+            c = None if cur is None else cur[f.t:f.t + k]
+            f.t += k
+            return o.run(k, current=c)[0]
+        f.t = 0
+        return f
+
+    r_gpu, s_gpu = _run_snapshots(gpu_run, steps, lambda: [net.get_state(k) for k in range(4)])
+    r_orc, s_orc = _run_snapshots(orc(onet), steps, lambda: onet.state)
+    r_64, s_64 = _run_snapshots(orc(o64), steps, lambda: o64.state)
+    assert r_gpu.shape == r_orc.shape == (steps, W)
+    # rasters bit-exact for the first 100 steps
+    assert np.array_equal(r_gpu[:100], r_orc[:100]), name
+    diff = np.nonzero(np.any(r_gpu != r_orc, axis=1))[0]
+    flip = int(diff[0]) if diff.size else steps
+    # state until the first flip: the last snapshot taken before it
+    snap_t = max([t for t in s_gpu if t <= flip], default=None)
+    if snap_t is not None:
+        for k in range(4):
+            a, b = s_gpu[snap_t][k][:n].astype(np.float64), s_orc[snap_t][k][:n].astype(np.float64)
+            scale = max(np.abs(b).max(), 1e-30)
+            assert np.allclose(a, b, rtol=1e-5, atol=1e-5 * scale), (name, k, snap_t)
+    # population statistics over the full run
+    rg, cg, ng = _rate_cv(r_gpu, n, dt_ms)
+    ro, co, no = _rate_cv(r_orc, n, dt_ms)
+    assert no > 1000, (name, no)
+    assert abs(rg - ro) <= 0.01 * ro, (name, rg, ro)
+    assert abs(cg - co) <= 0.01 * co, (name, cg, co)
+    # the FP64 twin: membrane error (max |dv| / max |v|) at step 50 and at the
+    # last snapshot before the first flip
+    d64 = np.nonzero(np.any(r_gpu != r_64, axis=1))[0]
+    flip64 = int(d64[0]) if d64.size else steps
+    t64 = max([t for t in s_gpu if t <= flip64], default=None)
+
+    def verr(t):
+        a, b = s_gpu[t][0][:n].astype(np.float64), s_64[t][0][:n]
+        return float(np.max(np.abs(a - b)) / max(np.abs(b).max(), 1e-30))
+    print(json.dumps({"workload": name, "steps": steps, "first_flip_vs_fp32_oracle": flip,
+                      "rate_hz": [rg, ro], "isi_cv": [cg, co], "spikes": [ng, no],
+                      "first_flip_vs_fp64": flip64, "v_rel_err_vs_fp64_step50": verr(SNAP),
+                      "v_rel_err_vs_fp64_before_flip": verr(t64) if t64 else None, "at_step": t64}))
+    assert flip64 >= SNAP, (name, flip64)
+    assert verr(SNAP) <= 1e-4, (name, verr(SNAP))
+    assert verr(t64) <= 1e-2, (name, t64, verr(t64))
+
+
+def test_izhikevich_1000(ctx):
+    net_ = izh_network(n=1000, seed=5)
+    n, steps = net_["n"], 1000
+    csr = sz.csr_from_synapses(n, 20, net_["src"], net_["tgt"], net_["w"], net_["d1"])
+    pn = np.zeros((12, n), np.float32)
+    pn[0], pn[1], pn[2], pn[3] = net_["a"], net_["b"], net_["c"], net_["d"]
+    pops = [sz.Pop(sz.IZHIKEVICH, 0, n, np.zeros(12, np.float32), per_unit=pn)]
+    st = [net_["v0"], net_["u0"], None, None]
+    net = sz.Network(ctx, n, 0, 20, pops, csr=csr, state=st, graph_chunk=50)
+    onet = oracle.OracleNet(n, 0, 20, pops, csr, state=st)
+    o64 = oracle.OracleNet(n, 0, 20, pops, csr, state=st, dtype=np.float64)
+    cur = thalamic(n, net_["ne"], steps, seed=9)
+    _check("izhikevich-1000", net, onet, o64, n, steps, 1.0, cur=cur)
+    net.close()
+
+
+def _if_balanced(seed=11):
+    rng = np.random.default_rng(seed)
+    n, ne, p_src = 4000, 3200, 1000
+    src, tgt, w, d1 = [], [], [], []
+    for s in range(n + p_src):
+        k = rng.binomial(n, 0.02)
+        t = rng.choice(n, k, replace=False)
+        src.append(np.full(k, s))
+        tgt.append(t)
+        if s < n:
+            w.append(np.full(k, 0.25 if s < ne else -2.25, np.float32))
+            d1.append(rng.integers(1, 101, k) + 1)  # user delay U{1..100} steps, stored +1
+        else:
+            w.append(np.full(k, 0.25, np.float32))
+            d1.append(np.full(k, 1))
+    src, tgt, w, d1 = (np.concatenate(x) for x in (src, tgt, w, d1))
+    pv = sz.fold_dt(sz.if_params(v_rest=-60, cm=0.2, tau_m=20, tau_refrac=5, tau_syn_E=5, tau_syn_I=10,
+                                 v_reset=-60, v_thresh=-50), 0.1)
+    pops = [sz.Pop(sz.IF_CURR_EXP, 0, n, pv),
+            sz.Pop(sz.POISSON, n, n + p_src, np.array([10.0 * 0.1e-3], np.float32), seed=77)]
+    v0 = np.concatenate([rng.uniform(-60, -50, n), np.zeros(p_src)]).astype(np.float32)
+    fr = np.concatenate([np.full(n, 1e4), np.zeros(p_src)]).astype(np.float32)
+    csr = sz.csr_from_synapses(n + p_src, 101, src, tgt, w, d1.astype(np.uint32))
+    return n, p_src, pops, csr, [v0, None, None, fr]
+
+
+def test_if_curr_exp_balanced_4000(ctx):
+    n, p, pops, csr, st = _if_balanced()
+    net = sz.Network(ctx, n, p, 101, pops, csr=csr, state=st, graph_chunk=50)
+    onet = oracle.OracleNet(n, p, 101, pops, csr, state=st)
+    o64 = oracle.OracleNet(n, p, 101, pops, csr, state=st, dtype=np.float64)
+    _check("if_curr_exp-4000", net, onet, o64, n, 10000, 0.1)
+    net.close()
+
+
+def test_if_cond_exp_100k(ctx):
+    """The benchmark's network builder (same populations, generator blocks,
+    weights, delays, Poisson rate and initial state) at 100k neurons."""
+    import bench
+    n, p, D, blocks, pops = bench.cond_config(100_000, 1000)
+    st = bench.init_state(n, p, 3)
+    net = sz.Network(ctx, n, p, D, pops, state=st, graph_chunk=50)
+    net.generate(blocks, seed=31)
+    csr = oracle.generate(blocks, 31, n + p, D)
+    onet = oracle.OracleNet(n, p, D, pops, csr, state=st)
+    o64 = oracle.OracleNet(n, p, D, pops, csr, state=st, dtype=np.float64)
+    _check("if_cond_exp-100k", net, onet, o64, n, 2000, 0.1)
+    net.close()
