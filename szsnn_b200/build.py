@@ -18,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libszsnn_cuda.so")
+REF_HOST = os.path.join(HERE, "szsnn_ref_host")  # C++ host on the drop-in kernel seam (csrc/ref_host.cpp)
 
 SOURCES = [
     "context.cu",
@@ -72,6 +73,13 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             subprocess.run(cmd, check=True)
     if force or _stale(LIB, objs):
         cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    host_src = os.path.join(CSRC, "ref_host.cpp")
+    if force or _stale(REF_HOST, [host_src, LIB, os.path.join(ROOT, "include", "szsnn_cuda.h")]):
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), host_src,
+               "-L", HERE, "-lszsnn_cuda", "-Wl,-rpath,$ORIGIN", "-o", REF_HOST]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

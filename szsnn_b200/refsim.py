@@ -117,6 +117,12 @@ class RefSimulation:
         neuron_vars = np.asarray(neuron_vars, dtype=np.float32)
         if neuron_params.shape[1] != PARAM_COUNT[mid] or neuron_vars.shape[1] != VAR_COUNT[mid]:
             raise ValueError("parameter / variable count does not match the model traits")
+        ctx_consts = getattr(getattr(backend, "ctx", None), "consts", None)
+        if ctx_consts is not None and tuple(ctx_consts.__getattribute__(f) for f, _ in consts._fields_) != \
+                tuple(consts.__getattribute__(f) for f, _ in consts._fields_):
+            # the drop-in kernels size their indexing by the context's constants
+            raise ValueError("layout constants differ from the context's: create the Context with the same "
+                             "max_partition_size / threads_per_group / warp_size / max_synaptic_delay")
         self.model = model
         self.backend = backend
         self.consts = consts

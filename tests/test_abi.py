@@ -94,3 +94,34 @@ def test_csr_bucketing_and_words():
     assert list(tg) == [1, 2, 2, 1, 0]
     ids = np.array([0, 5, 31, 32, 70])
     assert np.array_equal(sz.words_to_ids(sz.ids_to_words(ids, 80), 80), ids)
+
+
+def test_cpp_host_builds_and_checks_its_input(built, tmp_path):
+    """The C++ host on the kernel seam links against the library alone; input
+    errors are reported before any device work."""
+    from szsnn_b200.build import REF_HOST
+    r = subprocess.run([REF_HOST], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(b"NOTANETWORKFILE")
+    r = subprocess.run([REF_HOST, str(bad), str(tmp_path / "o.bin")], capture_output=True, text=True)
+    assert r.returncode == 1 and "not a network file" in r.stderr
+    out = subprocess.run(["ldd", REF_HOST], capture_output=True, text=True).stdout
+    assert "libszsnn_cuda.so" in out
+
+
+def test_reference_driver_rejects_mismatched_layout_constants(built):
+    """The drop-in kernels index with the context's layout constants, so a
+    layout built with other constants is refused before anything runs."""
+    class FakeCtx:
+        consts = L.LayoutConsts(1024, 256, 32, 64)
+
+    class FakeBackend:
+        ctx = FakeCtx()
+
+    n = 8
+    params = np.tile(sz.if_params()[:9], (n, 1))
+    vars_ = np.zeros((n, 4), np.float32)
+    with pytest.raises(ValueError, match="layout constants"):
+        sz.RefSimulation(FakeBackend(), L.LayoutConsts(256, 64, 32, 64), "IF_curr_exp", params, vars_,
+                         [0], [1], [0.5], [1])
