@@ -373,6 +373,81 @@ __device__ __forceinline__ int find_pop(const PopDev* pops, int npops, int64_t i
 // t+1, and block 0 does the per-step bookkeeping (spikes of step t-1 into the
 // statistics, slot t+1 emptied for update(t+1), events of step t's buffer
 // moved from pending to consumed).
+// Spike bookkeeping of one warp: group counters, raster word, compaction into
+// ring slot t (one atomic per spiking warp) and, in the overlapped order,
+// delivery of the spiking units' delay-1 buckets into step t+1's inputs.
+__device__ __forceinline__ void update_spikes(const NetDev& nd, long long t, int64_t id, bool spk, uint32_t lane,
+                                              uint32_t* __restrict__ out_words)
+{
+    if (spk && nd.group) atomicAdd(&nd.group_spikes[nd.group[id]], 1ull);
+    const uint32_t ball = __ballot_sync(0xffffffffu, spk);
+    const int64_t wd = id >> 5;
+    if (lane == 0 && out_words && wd < nd.words) out_words[wd] = ball;
+    if (ball) {
+        const int R = nd.D + 1;
+        const int64_t slot = t % R;
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&nd.ring_cnt[slot], (uint32_t)__popc(ball));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (spk) {
+            uint32_t rank = __popc(ball & ((1u << lane) - 1u));
+            uint32_t pos = base + rank;
+            if (pos < (uint32_t)nd.U) nd.ring_ids[slot * nd.U + pos] = (int32_t)id;
+            else dev_error(nd.err, SZSNN_DEV_RING_OVERFLOW, (uint32_t)slot);
+        }
+        if (nd.overlap) {  // m = 1 buckets of this warp's spiking units into step t+1's inputs
+            const InBuf nb = in_buf(nd, t + 1);
+            unsigned long long ra = 0, re = 0;
+            if (spk) {
+                ra = nd.row_ptr[id * nd.D];
+                re = nd.row_ptr[id * nd.D + 1];
+            }
+            uint32_t ev = 0;
+            for (uint32_t bits = ball; bits; bits &= bits - 1u) {
+                const int l = __ffs(bits) - 1;
+                const unsigned long long a = __shfl_sync(0xffffffffu, ra, l);
+                const unsigned long long e = __shfl_sync(0xffffffffu, re, l);
+                for (unsigned long long q = a + lane; q < e; q += 32) deliver(nd, nb, nd.syn[q], ev);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
+            if (lane == 0 && ev) atomicAdd(&nd.stats[2 + ((t + 1) & 1)], (unsigned long long)ev);
+        }
+    }
+}
+
+// One unit of a block that lies inside one population with shared parameters:
+// the model and the accumulation mode are compile-time, the parameters are
+// read from the staged population (broadcast shared-memory loads).  Same
+// arithmetic as the generic path.
+template <int MODEL, bool FIXED>
+__device__ __forceinline__ bool update_unit_shared(const NetDev& nd, const InBuf& inb, const PopDev& P, int64_t id,
+                                                   long long t, float& v, float& g1, float& g2, float& fr,
+                                                   float in_e, float in_i, long long fxe, long long fxi, float i_ext,
+                                                   bool f)
+{
+    if (MODEL == SZSNN_POISSON) return sz_poisson_fires(P.seed, id - P.begin, t, P.p[0]) || f;
+    if (FIXED) {
+        in_e = __ll2float_rn(fxe) * (1.0f / 4294967296.0f);
+        in_i = __ll2float_rn(fxi) * (1.0f / 4294967296.0f);
+        inb.fe[id] = 0;
+        inb.fi[id] = 0;
+    } else {
+        inb.e[id] = 0.0f;
+        inb.i[id] = 0.0f;
+    }
+    if (nd.dbg_in_e) { nd.dbg_in_e[id] = in_e; nd.dbg_in_i[id] = in_i; }
+    const SharedParams sp{P.p};
+    bool spk;
+    if (MODEL == SZSNN_IF_CURR_EXP) spk = sz_if_curr_exp(sp, v, g1, g2, fr, in_e, in_i, i_ext, f, sp(12), sp(13));
+    else if (MODEL == SZSNN_IF_COND_EXP) spk = sz_if_cond_exp(sp, v, g1, g2, fr, in_e, in_i, i_ext, f, sp(12), sp(13));
+    else spk = sz_izhikevich(sp, v, g1, in_e, in_i, i_ext, f, (P.flags & SZSNN_POP_IZH_HALF_STEPS) != 0);
+    nd.st0[id] = v;
+    nd.st1[id] = g1;
+    if (MODEL != SZSNN_IZHIKEVICH) { nd.st2[id] = g2; nd.st3[id] = fr; }
+    return spk;
+}
+
 __device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk, const uint32_t* __restrict__ forced,
                                             const float* __restrict__ current, uint32_t* __restrict__ out_words)
 {
@@ -425,81 +500,83 @@ __device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk
         nd.stats[2 + (t & 1)] = 0;
         atomicAdd(&nd.stats[0], pend);
     }
-    const PopDev* pd = nullptr;
-    if (unit) {
-        const int np = s_np;
-        if (np >= 0) {
-            for (int i = 0; i < np; ++i)
-                if (id >= s_pop[i].begin && id < s_pop[i].end) { pd = &s_pop[i]; break; }
-        } else {
-            const int pi = find_pop(nd.pops, nd.npops, id);
-            if (pi >= 0 && id < nd.pops[pi].end) pd = &nd.pops[pi];
+    // a block inside one staged population with shared parameters and a model
+    // the specialised update covers (decided from shared memory, the same for
+    // every thread of the block)
+    int single = -1;
+    if (s_np > 0) {
+        const int64_t b1 = min(b0 + (int64_t)blockDim.x, nd.U);
+        for (int i = 0; i < s_np; ++i) {
+            const PopDev& q = s_pop[i];
+            if (q.begin <= b0 && q.end >= b1 && !q.pn &&
+                (q.model == SZSNN_IF_CURR_EXP || q.model == SZSNN_IF_COND_EXP || q.model == SZSNN_IZHIKEVICH ||
+                 q.model == SZSNN_POISSON)) {
+                single = i;
+                break;
+            }
         }
     }
     bool spk = false;
-    if (pd) {
-        const int model = pd->model;
-        if (neuron) {
-            if (nd.acc_mode == SZSNN_ACC_FIXED) {
-                in_e = __ll2float_rn(fxe) * (1.0f / 4294967296.0f);
-                in_i = __ll2float_rn(fxi) * (1.0f / 4294967296.0f);
-                inb.fe[id] = 0;
-                inb.fi[id] = 0;
+    if (single >= 0) {
+        if (unit) {
+            const PopDev& P = s_pop[single];
+            const bool fx = nd.acc_mode == SZSNN_ACC_FIXED;
+#define SZ_FAST(M)                                                                                         \
+    spk = fx ? update_unit_shared<M, true>(nd, inb, P, id, t, v, g1, g2, fr, in_e, in_i, fxe, fxi, i_ext, f) \
+             : update_unit_shared<M, false>(nd, inb, P, id, t, v, g1, g2, fr, in_e, in_i, fxe, fxi, i_ext, f)
+            switch (P.model) {
+            case SZSNN_IF_CURR_EXP: SZ_FAST(SZSNN_IF_CURR_EXP); break;
+            case SZSNN_IF_COND_EXP: SZ_FAST(SZSNN_IF_COND_EXP); break;
+            case SZSNN_IZHIKEVICH: SZ_FAST(SZSNN_IZHIKEVICH); break;
+            default: SZ_FAST(SZSNN_POISSON); break;
+            }
+#undef SZ_FAST
+        }
+    } else {
+        const PopDev* pd = nullptr;
+        if (unit) {
+            const int np = s_np;
+            if (np >= 0) {
+                for (int i = 0; i < np; ++i)
+                    if (id >= s_pop[i].begin && id < s_pop[i].end) { pd = &s_pop[i]; break; }
             } else {
-                inb.e[id] = 0.0f;
-                inb.i[id] = 0.0f;
+                const int pi = find_pop(nd.pops, nd.npops, id);
+                if (pi >= 0 && id < nd.pops[pi].end) pd = &nd.pops[pi];
             }
-            if (nd.dbg_in_e) { nd.dbg_in_e[id] = in_e; nd.dbg_in_i[id] = in_i; }
-            if (pd->pn) spk = run_neuron(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, model, pd->flags,
-                                         v, g1, g2, fr, in_e, in_i, i_ext, f);
-            else spk = run_neuron(SharedParams{pd->p}, model, pd->flags, v, g1, g2, fr, in_e, in_i, i_ext, f);
-            st0[id] = v;
-            st1[id] = g1;
-            if (model != SZSNN_IZHIKEVICH) { st2[id] = g2; st3[id] = fr; }
-        } else if (model == SZSNN_POISSON) {
-            const float prob = pd->pn ? pd->pn[id - pd->begin] : pd->p[0];
-            spk = sz_poisson_fires(pd->seed, id - pd->begin, t, prob) || f;
-        } else if (model == SZSNN_CONST_RATE) {
-            if (pd->pn) spk = sz_const_rate(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, v, f);
-            else spk = sz_const_rate(SharedParams{pd->p}, v, f);
-            st0[id] = v;
+        }
+        if (pd) {
+            const int model = pd->model;
+            if (neuron) {
+                if (nd.acc_mode == SZSNN_ACC_FIXED) {
+                    in_e = __ll2float_rn(fxe) * (1.0f / 4294967296.0f);
+                    in_i = __ll2float_rn(fxi) * (1.0f / 4294967296.0f);
+                    inb.fe[id] = 0;
+                    inb.fi[id] = 0;
+                } else {
+                    inb.e[id] = 0.0f;
+                    inb.i[id] = 0.0f;
+                }
+                if (nd.dbg_in_e) { nd.dbg_in_e[id] = in_e; nd.dbg_in_i[id] = in_i; }
+                if (pd->pn) spk = run_neuron(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, model, pd->flags,
+                                             v, g1, g2, fr, in_e, in_i, i_ext, f);
+                else spk = run_neuron(SharedParams{pd->p}, model, pd->flags, v, g1, g2, fr, in_e, in_i, i_ext, f);
+                st0[id] = v;
+                st1[id] = g1;
+                if (model != SZSNN_IZHIKEVICH) { st2[id] = g2; st3[id] = fr; }
+            } else if (model == SZSNN_POISSON) {
+                const float prob = pd->pn ? pd->pn[id - pd->begin] : pd->p[0];
+                spk = sz_poisson_fires(pd->seed, id - pd->begin, t, prob) || f;
+            } else if (model == SZSNN_CONST_RATE) {
+                if (pd->pn) spk = sz_const_rate(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, v, f);
+                else spk = sz_const_rate(SharedParams{pd->p}, v, f);
+                st0[id] = v;
+            }
         }
     }
-    if (spk && nd.group) atomicAdd(&nd.group_spikes[nd.group[id]], 1ull);
-    const uint32_t ball = __ballot_sync(0xffffffffu, spk);
-    const int64_t wd = id >> 5;
-    if (lane == 0 && out_words && wd < nd.words) out_words[wd] = ball;
-    if (ball) {
-        const int R = nd.D + 1;
-        const int64_t slot = t % R;
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&nd.ring_cnt[slot], (uint32_t)__popc(ball));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (spk) {
-            uint32_t rank = __popc(ball & ((1u << lane) - 1u));
-            uint32_t pos = base + rank;
-            if (pos < (uint32_t)nd.U) nd.ring_ids[slot * nd.U + pos] = (int32_t)id;
-            else dev_error(nd.err, SZSNN_DEV_RING_OVERFLOW, (uint32_t)slot);
-        }
-        if (nd.overlap) {  // m = 1 buckets of this warp's spiking units into step t+1's inputs
-            const InBuf nb = in_buf(nd, t + 1);
-            unsigned long long ra = 0, re = 0;
-            if (spk) {
-                ra = nd.row_ptr[id * nd.D];
-                re = nd.row_ptr[id * nd.D + 1];
-            }
-            uint32_t ev = 0;
-            for (uint32_t bits = ball; bits; bits &= bits - 1u) {
-                const int l = __ffs(bits) - 1;
-                const unsigned long long a = __shfl_sync(0xffffffffu, ra, l);
-                const unsigned long long e = __shfl_sync(0xffffffffu, re, l);
-                for (unsigned long long q = a + lane; q < e; q += 32) deliver(nd, nb, nd.syn[q], ev);
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
-            if (lane == 0 && ev) atomicAdd(&nd.stats[2 + ((t + 1) & 1)], (unsigned long long)ev);
-        }
-    }
+    // one call site for every lane: the epilogue's warp collectives are reached
+    // by the whole warp at the same instruction
+    __syncwarp();
+    update_spikes(nd, t, id, spk, lane, out_words);
 }
 
 __global__ void __launch_bounds__(1024) k_update(NetDev nd, int k_off, const uint32_t* __restrict__ forced,
