@@ -51,6 +51,8 @@ extern "C" {
 #define SZSNN_DEV_RING_OVERFLOW  3  /* native spike ring slot full                    */
 #define SZSNN_DEV_NONFINITE      4  /* NaN/Inf found by szsnn_net_check_finite        */
 #define SZSNN_DEV_BAD_DELAY      5  /* delay outside 1..max_delay                     */
+#define SZSNN_DEV_STEP_PARITY    6  /* launch parity disagrees with the step counter  */
+#define SZSNN_DEV_WAIT_TIMEOUT   7  /* a bounded wait for a bulk copy ran out         */
 
 typedef struct szsnn_ctx szsnn_ctx;
 typedef struct szsnn_net szsnn_net;
@@ -324,7 +326,8 @@ int szsnn_net_profile_step(szsnn_net* net, int64_t steps, double* propagate_ms, 
 int szsnn_net_timing(szsnn_net* net, double* propagate_ms, double* update_ms, double* total_ms);
 /* launch shapes: propagate mode 0 = `group` lanes per (delay, spike) bucket
  * segment (4/8/16/32), mode 1 = warp-flattened walk over `group` items per
- * warp (8/16/32); propagate grid blocks (0 = 16 per SM); update block size */
+ * warp (8/16/32); propagate grid blocks (0 = 16 per SM); update block size
+ * (threads, a multiple of 32 in 32..256; each thread updates 4 units) */
 int szsnn_net_set_tuning(szsnn_net* net, int propagate_mode, int group, int propagate_blocks, int update_block);
 /* Step order.  1 (default): overlapped -- input buffers double-buffered by
  * step parity, delivery of delays >= 2 into step t+1 runs on a second stream

@@ -17,7 +17,7 @@ import os
 
 PROPAGATE = [(0, 8, 16), (0, 16, 8), (0, 16, 16), (0, 16, 32), (0, 32, 8), (0, 32, 16),
              (1, 8, 8), (1, 8, 16), (1, 16, 16), (1, 16, 32), (1, 32, 16)]  # classic: (mode, group, blocks/SM)
-UPDATE = [128, 256, 512]
+UPDATE = [64, 128, 256]
 FAR = [(0, 16), (0, 8), (1, 8), (1, 16), (1, 32)]        # overlapped delivery: (mode, group)
 FAR_THREADS_PER_SM = [256, 512, 1024, 2048, 4096]
 

@@ -38,6 +38,9 @@
 // slots 0..11 as szsnn_pop_desc; 12, 13 = 1 - 1/tau_syn_E, 1 - 1/tau_syn_I
 // (IF models), computed once on the host with the same fp32 operations
 #define POP_SLOTS 16
+#define INLINE_POPS 4
+#define UPD_UPT 4        // units per update thread, strided by the block size
+#define UPD_MAX_BLOCK 256  // update threads per block (the step kernel's block too)
 struct PopDev {
     int32_t model;
     uint32_t flags;
@@ -78,6 +81,9 @@ struct NetDev {
     const int32_t* group;                  // per-unit group or null
     unsigned long long* group_spikes;      // [n_groups]
     const int2* blk_pop;                   // per update block: (first overlapping pop, count)
+    uint32_t par0;                         // parity of the step counter when the launch runs
+    int32_t ib_lo[INLINE_POPS], ib_hi[INLINE_POPS];  // update blocks [lo, hi) lying inside slot i (empty: none)
+    PopDev ipop[INLINE_POPS];              // populations with shared parameters, by value in the kernel parameters
 };
 
 struct szsnn_net {
@@ -88,11 +94,12 @@ struct szsnn_net {
     int32_t npops = 0;
     std::vector<szsnn_pop_desc> pops;
     PopDev* d_pops = nullptr;
+    std::vector<PopDev> h_pops;            // the device table's host copy (kernel-parameter table)
     float* d_pn = nullptr;                 // all per-unit parameter arrays, back to back
     int32_t* d_group = nullptr;
     unsigned long long* d_group_spikes = nullptr;
     int32_t n_groups = 0;
-    int2* d_blk_pop = nullptr;             // sized for 32-thread blocks, filled for upd_block
+    int2* d_blk_pop = nullptr;             // per update-block tile: sized for 32-thread blocks, filled for upd_block
     uint64_t n_syn = 0;
     unsigned long long* d_row_ptr = nullptr;
     int2* d_syn = nullptr;
@@ -115,7 +122,7 @@ struct szsnn_net {
     cudaStream_t copy_st = nullptr;      // host <-> device copies of szsnn_net_run
     cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {};
     bool overlap = true;
-    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;  // (steps, io flags, stage parity)
+    std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;  // (steps, io flags, stage, step parity)
     int64_t steps_done = 0;
     uint64_t graph_launches = 0, kernel_launches = 0;
     int prop_mode = 0, prop_group = 16, prop_blocks = 0, upd_block = 256;
@@ -167,6 +174,12 @@ __device__ __forceinline__ InBuf in_buf(const NetDev& nd, long long t)
 {
     if (nd.overlap && (t & 1)) return InBuf{nd.in_e1, nd.in_i1, nd.fx_e1, nd.fx_i1};
     return InBuf{nd.in_e, nd.in_i, nd.fx_e, nd.fx_i};
+}
+
+// the same buffers from the host-known parity (no wait for the step counter)
+__device__ __forceinline__ InBuf in_buf_k(const NetDev& nd, int k_off)
+{
+    return in_buf(nd, (long long)((nd.par0 + (uint32_t)k_off) & 1u));
 }
 
 // one synapse into the exc / inh input of its target (weight sign picks the
@@ -269,7 +282,7 @@ __device__ __forceinline__ void propagate_grouped(const NetDev& nd, int k_off, i
 }
 
 template <int G>
-__global__ void __launch_bounds__(256) k_propagate(NetDev nd, int k_off, int m_lo, uint32_t pf)
+__global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ NetDev nd, int k_off, int m_lo, uint32_t pf)
 {
     propagate_grouped<G>(nd, k_off, m_lo, pf, blockIdx.x, gridDim.x);
 }
@@ -346,7 +359,7 @@ __device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int 
 }
 
 template <int IPW>
-__global__ void __launch_bounds__(256) k_propagate_flat(NetDev nd, int k_off, int m_lo, uint32_t pf)
+__global__ void __launch_bounds__(256) k_propagate_flat(const __grid_constant__ NetDev nd, int k_off, int m_lo, uint32_t pf)
 {
     propagate_flat<IPW>(nd, k_off, m_lo, pf, blockIdx.x, gridDim.x);
 }
@@ -364,15 +377,6 @@ __device__ __forceinline__ int find_pop(const PopDev* pops, int npops, int64_t i
 
 #define UPD_BLOCK_POPS 8
 
-// One thread per unit.  Thread 0 stages the populations overlapping the
-// block (and the step counter) in shared memory while every thread already
-// has its state loads in flight, so each thread's chain of dependent global
-// accesses is: state / input loads -> model arithmetic -> stores.
-// Overlapped stepping: the inputs of step t are the parity buffer of t; the
-// warps with spikes deliver their units' m = 1 buckets into the buffer of
-// t+1, and block 0 does the per-step bookkeeping (spikes of step t-1 into the
-// statistics, slot t+1 emptied for update(t+1), events of step t's buffer
-// moved from pending to consumed).
 // Spike bookkeeping of one warp: group counters, raster word, compaction into
 // ring slot t (one atomic per spiking warp) and, in the overlapped order,
 // delivery of the spiking units' delay-1 buckets into step t+1's inputs.
@@ -416,26 +420,150 @@ __device__ __forceinline__ void update_spikes(const NetDev& nd, long long t, int
     }
 }
 
-// One unit of a block that lies inside one population with shared parameters:
-// the model and the accumulation mode are compile-time, the parameters are
-// read from the staged population (broadcast shared-memory loads).  Same
-// arithmetic as the generic path.
-template <int MODEL, bool FIXED>
-__device__ __forceinline__ bool update_unit_shared(const NetDev& nd, const InBuf& inb, const PopDev& P, int64_t id,
-                                                   long long t, float& v, float& g1, float& g2, float& fr,
-                                                   float in_e, float in_i, long long fxe, long long fxi, float i_ext,
-                                                   bool f)
+// Per-step bookkeeping of the overlapped order, by one thread of update block
+// 0: spikes of step t-1 into the statistics, ring slot t+1 emptied for
+// update(t+1) (it held step t-D, read last by the delivery into step t),
+// events of step t's buffer moved from pending to consumed.
+__device__ __forceinline__ void step_bookkeeping(const NetDev& nd, long long t)
 {
-    if (MODEL == SZSNN_POISSON) return sz_poisson_fires(P.seed, id - P.begin, t, P.p[0]) || f;
+    const int R = nd.D + 1;
+    if (t >= 1) atomicAdd(&nd.stats[1], (unsigned long long)nd.ring_cnt[(t - 1) % R]);
+    nd.ring_cnt[(t + 1) % R] = 0;
+    const unsigned long long pend = nd.stats[2 + (t & 1)];
+    nd.stats[2 + (t & 1)] = 0;
+    atomicAdd(&nd.stats[0], pend);
+}
+
+// Unit state and inputs of the generic update, loaded before the block's
+// population lookup so the loads of a warp are in flight together.
+struct UnitIn {
+    float v, g1, g2, fr, in_e, in_i, i_ext;
+    long long fxe, fxi;
+    bool f;
+};
+
+// ---- inline tiles: blocks inside one population of the parameter table
+//
+// The block's tile of T = UPD_UPT * blockDim.x units is brought into shared
+// memory by bulk copies (one per state / input array, issued by one thread,
+// completing on an mbarrier), so the bytes in flight are bounded by shared
+// memory rather than by registers.  Each thread then updates units
+// j * blockDim.x + threadIdx.x of the tile from shared memory, with the
+// population's parameters as constant-bank operands (slot and model
+// compile-time), and stores state and cleared inputs straight to global.
+// Dynamic shared memory: mbarrier at 0, arrays from byte 16: st0..st3 (T
+// floats each), then the exc / inh inputs (T floats or T int64 each).
+__host__ __device__ __forceinline__ size_t tile_smem_bytes(int64_t T, bool fixed)
+{
+    return 16 + (size_t)T * (16 + (fixed ? 16 : 8));
+}
+
+struct TileSmem {
+    uint64_t* bar;
+    float* st[4];
+    float* ie;
+    float* ii;
+    long long* fe;
+    long long* fi;
+};
+
+__device__ __forceinline__ TileSmem tile_smem(unsigned char* base, uint32_t T, bool fixed)
+{
+    TileSmem m;
+    m.bar = reinterpret_cast<uint64_t*>(base);
+    float* f = reinterpret_cast<float*>(base + 16);
+    for (int k = 0; k < 4; ++k) m.st[k] = f + (size_t)k * T;
+    m.ie = f + 4 * (size_t)T;
+    m.ii = f + 5 * (size_t)T;
+    m.fe = reinterpret_cast<long long*>(f + 4 * (size_t)T);
+    m.fi = m.fe + T;
+    return m;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+    return ok != 0u;
+}
+
+// bounded wait for phase 0 of the tile's mbarrier
+__device__ __forceinline__ bool tile_wait(uint64_t* bar)
+{
+    for (int i = 0; i < (1 << 20); ++i)
+        if (mbar_try_wait(bar, 0u)) return true;
+    return false;
+}
+
+// Issue the tile's bulk copies (thread 0) and wait for them (all threads).
+// Model M decides which arrays a unit reads; Poisson tiles read none.
+template <int MODEL, bool FIXED>
+__device__ __forceinline__ bool tile_load(const NetDev& nd, const InBuf& inb, int64_t tile0, uint32_t T,
+                                          const TileSmem& sm)
+{
+    if (MODEL == SZSNN_POISSON) return true;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(sm.bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int64_t n = min((int64_t)T, nd.U - tile0);  // the tile lies inside a neuron population
+        const uint32_t b4 = (uint32_t)((n * 4 + 15) & ~(int64_t)15);
+        const uint32_t b8 = (uint32_t)((n * 8 + 15) & ~(int64_t)15);
+        const int nst = MODEL == SZSNN_IZHIKEVICH ? 2 : 4;
+        const uint32_t total = (uint32_t)nst * b4 + 2u * (FIXED ? b8 : b4);
+        asm volatile("{\n .reg .b64 s;\n mbarrier.arrive.expect_tx.shared::cta.b64 s, [%0], %1;\n}"
+                     :: "r"(smem_addr(sm.bar)), "r"(total) : "memory");
+        float* const gst[4] = {nd.st0, nd.st1, nd.st2, nd.st3};
+        for (int k = 0; k < nst; ++k) bulk_load(sm.st[k], gst[k] + tile0, b4, sm.bar);
+        if (FIXED) {
+            bulk_load(sm.fe, inb.fe + tile0, b8, sm.bar);
+            bulk_load(sm.fi, inb.fi + tile0, b8, sm.bar);
+        } else {
+            bulk_load(sm.ie, inb.e + tile0, b4, sm.bar);
+            bulk_load(sm.ii, inb.i + tile0, b4, sm.bar);
+        }
+    }
+    if (tile_wait(sm.bar)) return true;
+    // the copies did not complete in time: report, wait once more so none is
+    // still writing shared memory when the block leaves, skip the tile
+    if (threadIdx.x == 0) dev_error(nd.err, SZSNN_DEV_WAIT_TIMEOUT, (uint32_t)tile0);
+    tile_wait(sm.bar);
+    return false;
+}
+
+// one unit of an inline tile, from shared memory (u = index in the tile)
+template <int MODEL, bool FIXED>
+__device__ __forceinline__ bool tile_unit(const NetDev& nd, const PopDev& P, const InBuf& inb, const TileSmem& sm,
+                                          uint32_t id, uint32_t u, long long t, const uint32_t* __restrict__ forced,
+                                          const float* __restrict__ current)
+{
+    const bool f = forced ? ((forced[id >> 5] >> (id & 31)) & 1u) != 0u : false;
+    if (MODEL == SZSNN_POISSON) return sz_poisson_fires(P.seed, (int64_t)id - P.begin, t, P.p[0]) || f;
+    float v = sm.st[0][u], g1 = sm.st[1][u], g2 = 0.0f, fr = 0.0f, in_e, in_i;
+    if (MODEL != SZSNN_IZHIKEVICH) { g2 = sm.st[2][u]; fr = sm.st[3][u]; }
     if (FIXED) {
-        in_e = __ll2float_rn(fxe) * (1.0f / 4294967296.0f);
-        in_i = __ll2float_rn(fxi) * (1.0f / 4294967296.0f);
+        in_e = __ll2float_rn(sm.fe[u]) * (1.0f / 4294967296.0f);
+        in_i = __ll2float_rn(sm.fi[u]) * (1.0f / 4294967296.0f);
         inb.fe[id] = 0;
         inb.fi[id] = 0;
     } else {
+        in_e = sm.ie[u];
+        in_i = sm.ii[u];
         inb.e[id] = 0.0f;
         inb.i[id] = 0.0f;
     }
+    const float i_ext = current ? current[id] : 0.0f;
     if (nd.dbg_in_e) { nd.dbg_in_e[id] = in_e; nd.dbg_in_i[id] = in_i; }
     const SharedParams sp{P.p};
     bool spk;
@@ -448,17 +576,70 @@ __device__ __forceinline__ bool update_unit_shared(const NetDev& nd, const InBuf
     return spk;
 }
 
-__device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk, const uint32_t* __restrict__ forced,
-                                            const float* __restrict__ current, uint32_t* __restrict__ out_words)
+// The whole inline tile with population slot PI and model MODEL: bulk load,
+// then the UPD_UPT sub-tiles, each ending in the spike epilogue.
+template <int MODEL, bool FIXED, int PI>
+__device__ __forceinline__ void tile_run(const NetDev& nd, const InBuf& inb, int64_t tile0, long long t,
+                                        const uint32_t* __restrict__ forced, const float* __restrict__ current,
+                                        uint32_t* __restrict__ out_words, unsigned char* smem)
+{
+    const uint32_t bs = blockDim.x, T = UPD_UPT * bs, lane = threadIdx.x & 31;
+    const TileSmem sm = tile_smem(smem, T, FIXED);
+    const bool ok = tile_load<MODEL, FIXED>(nd, inb, tile0, T, sm);
+    const PopDev& P = nd.ipop[PI];
+#pragma unroll 1
+    for (int j = 0; j < UPD_UPT; ++j) {
+        const uint32_t u = (uint32_t)j * bs + threadIdx.x;
+        const int64_t id = tile0 + u;
+        bool spk = false;
+        if (ok && id < nd.U) spk = tile_unit<MODEL, FIXED>(nd, P, inb, sm, (uint32_t)id, u, t, forced, current);
+        __syncwarp();
+        update_spikes(nd, t, id, spk, lane, out_words);
+    }
+}
+
+template <bool FIXED, int PI>
+__device__ __forceinline__ void tile_run_pop(const NetDev& nd, const InBuf& inb, int64_t tile0, long long t,
+                                            const uint32_t* __restrict__ forced, const float* __restrict__ current,
+                                            uint32_t* __restrict__ out_words, unsigned char* smem)
+{
+    switch (nd.ipop[PI].model) {
+    case SZSNN_IF_CURR_EXP: tile_run<SZSNN_IF_CURR_EXP, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem); break;
+    case SZSNN_IF_COND_EXP: tile_run<SZSNN_IF_COND_EXP, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem); break;
+    case SZSNN_IZHIKEVICH: tile_run<SZSNN_IZHIKEVICH, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem); break;
+    default: tile_run<SZSNN_POISSON, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem); break;
+    }
+}
+
+template <bool FIXED>
+__device__ __forceinline__ void tile_run_slot(const NetDev& nd, int slot, const InBuf& inb, int64_t tile0, long long t,
+                                             const uint32_t* __restrict__ forced, const float* __restrict__ current,
+                                             uint32_t* __restrict__ out_words, unsigned char* smem)
+{
+    static_assert(INLINE_POPS == 4, "one case per parameter-table slot");
+    switch (slot) {
+    case 0: tile_run_pop<FIXED, 0>(nd, inb, tile0, t, forced, current, out_words, smem); break;
+    case 1: tile_run_pop<FIXED, 1>(nd, inb, tile0, t, forced, current, out_words, smem); break;
+    case 2: tile_run_pop<FIXED, 2>(nd, inb, tile0, t, forced, current, out_words, smem); break;
+    default: tile_run_pop<FIXED, 3>(nd, inb, tile0, t, forced, current, out_words, smem); break;
+    }
+}
+
+// Generic update: the block stages the populations overlapping its tile in
+// shared memory once, then each thread finds the population of each of its
+// units.  Handles per-unit parameters, Const_rate sources, tiles spanning
+// populations and population tables larger than the parameter table.
+struct StagedPops {
+    const PopDev* pop;  // shared-memory copy
+    int np;             // populations staged, -1 when more overlap the tile (global lookup)
+};
+
+__device__ __forceinline__ StagedPops stage_pops(const NetDev& nd, int blk)
 {
     __shared__ PopDev s_pop[UPD_BLOCK_POPS];
-    __shared__ int s_np;  // populations staged, -1 when more overlap the block (global lookup)
-    __shared__ long long s_t;
-    const int64_t b0 = (int64_t)blk * blockDim.x;
-    const int64_t id = b0 + threadIdx.x;
-    const uint32_t lane = threadIdx.x & 31;
-    // populations overlapping the block: the whole table when it is small, else
-    // the host-computed (first, count) of this block; one cooperative copy
+    __shared__ int s_np;
+    // populations overlapping the tile: the whole table when it is small, else
+    // the host-computed (first, count) of this tile; one cooperative copy
     int first = 0, np = nd.npops;
     if (np > UPD_BLOCK_POPS) {
         const int2 fc = nd.blk_pop[blk];
@@ -470,116 +651,125 @@ __device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk
         unsigned long long* dst = reinterpret_cast<unsigned long long*>(s_pop);
         for (int w = threadIdx.x; w < np * (int)(sizeof(PopDev) / 8); w += blockDim.x) dst[w] = src[w];
     }
-    if (threadIdx.x == 0) { s_np = np; s_t = *nd.clock + k_off; }
-    const int64_t tq = (int64_t)(*nd.clock + k_off);  // all threads: selects the input buffer
-    const InBuf inb = in_buf(nd, tq);
-    float* __restrict__ st0 = nd.st0;
-    float* __restrict__ st1 = nd.st1;
-    float* __restrict__ st2 = nd.st2;
-    float* __restrict__ st3 = nd.st3;
-    const bool unit = id < nd.U, neuron = id < nd.N;
-    float v = 0.0f, g1 = 0.0f, g2 = 0.0f, fr = 0.0f, in_e = 0.0f, in_i = 0.0f, i_ext = 0.0f;
-    long long fxe = 0, fxi = 0;
-    if (unit) v = st0[id];
-    if (neuron) {
-        g1 = st1[id];
-        g2 = st2[id];
-        fr = st3[id];
-        if (nd.acc_mode == SZSNN_ACC_FIXED) { fxe = inb.fe[id]; fxi = inb.fi[id]; }
-        else { in_e = inb.e[id]; in_i = inb.i[id]; }
-        if (current) i_ext = current[id];
-    }
-    const bool f = (forced && unit) ? ((forced[id >> 5] >> (id & 31)) & 1u) : false;
+    if (threadIdx.x == 0) s_np = np;
     __syncthreads();
-    const long long t = s_t;
-    if (nd.overlap && blk == 0 && threadIdx.x == 0) {
-        const int R = nd.D + 1;
-        if (t >= 1) atomicAdd(&nd.stats[1], (unsigned long long)nd.ring_cnt[(t - 1) % R]);
-        nd.ring_cnt[(t + 1) % R] = 0;  // held step t-D, read last by the delivery into step t
-        const unsigned long long pend = nd.stats[2 + (t & 1)];
-        nd.stats[2 + (t & 1)] = 0;
-        atomicAdd(&nd.stats[0], pend);
-    }
-    // a block inside one staged population with shared parameters and a model
-    // the specialised update covers (decided from shared memory, the same for
-    // every thread of the block)
-    int single = -1;
-    if (s_np > 0) {
-        const int64_t b1 = min(b0 + (int64_t)blockDim.x, nd.U);
-        for (int i = 0; i < s_np; ++i) {
-            const PopDev& q = s_pop[i];
-            if (q.begin <= b0 && q.end >= b1 && !q.pn &&
-                (q.model == SZSNN_IF_CURR_EXP || q.model == SZSNN_IF_COND_EXP || q.model == SZSNN_IZHIKEVICH ||
-                 q.model == SZSNN_POISSON)) {
-                single = i;
-                break;
-            }
+    return StagedPops{s_pop, s_np};
+}
+
+__device__ __forceinline__ bool update_generic(const NetDev& nd, const StagedPops& sp_, int64_t id, const InBuf& inb,
+                                               long long t, UnitIn& a)
+{
+    const bool unit = id < nd.U, neuron = id < nd.N;
+    const PopDev* pd = nullptr;
+    if (unit) {
+        if (sp_.np >= 0) {
+            for (int i = 0; i < sp_.np; ++i)
+                if (id >= sp_.pop[i].begin && id < sp_.pop[i].end) { pd = &sp_.pop[i]; break; }
+        } else {
+            const int pi = find_pop(nd.pops, nd.npops, id);
+            if (pi >= 0 && id < nd.pops[pi].end) pd = &nd.pops[pi];
         }
     }
     bool spk = false;
-    if (single >= 0) {
-        if (unit) {
-            const PopDev& P = s_pop[single];
-            const bool fx = nd.acc_mode == SZSNN_ACC_FIXED;
-#define SZ_FAST(M)                                                                                         \
-    spk = fx ? update_unit_shared<M, true>(nd, inb, P, id, t, v, g1, g2, fr, in_e, in_i, fxe, fxi, i_ext, f) \
-             : update_unit_shared<M, false>(nd, inb, P, id, t, v, g1, g2, fr, in_e, in_i, fxe, fxi, i_ext, f)
-            switch (P.model) {
-            case SZSNN_IF_CURR_EXP: SZ_FAST(SZSNN_IF_CURR_EXP); break;
-            case SZSNN_IF_COND_EXP: SZ_FAST(SZSNN_IF_COND_EXP); break;
-            case SZSNN_IZHIKEVICH: SZ_FAST(SZSNN_IZHIKEVICH); break;
-            default: SZ_FAST(SZSNN_POISSON); break;
-            }
-#undef SZ_FAST
-        }
-    } else {
-        const PopDev* pd = nullptr;
-        if (unit) {
-            const int np = s_np;
-            if (np >= 0) {
-                for (int i = 0; i < np; ++i)
-                    if (id >= s_pop[i].begin && id < s_pop[i].end) { pd = &s_pop[i]; break; }
+    if (pd) {
+        const int model = pd->model;
+        if (neuron) {
+            if (nd.acc_mode == SZSNN_ACC_FIXED) {
+                a.in_e = __ll2float_rn(a.fxe) * (1.0f / 4294967296.0f);
+                a.in_i = __ll2float_rn(a.fxi) * (1.0f / 4294967296.0f);
+                inb.fe[id] = 0;
+                inb.fi[id] = 0;
             } else {
-                const int pi = find_pop(nd.pops, nd.npops, id);
-                if (pi >= 0 && id < nd.pops[pi].end) pd = &nd.pops[pi];
+                inb.e[id] = 0.0f;
+                inb.i[id] = 0.0f;
             }
-        }
-        if (pd) {
-            const int model = pd->model;
-            if (neuron) {
-                if (nd.acc_mode == SZSNN_ACC_FIXED) {
-                    in_e = __ll2float_rn(fxe) * (1.0f / 4294967296.0f);
-                    in_i = __ll2float_rn(fxi) * (1.0f / 4294967296.0f);
-                    inb.fe[id] = 0;
-                    inb.fi[id] = 0;
-                } else {
-                    inb.e[id] = 0.0f;
-                    inb.i[id] = 0.0f;
-                }
-                if (nd.dbg_in_e) { nd.dbg_in_e[id] = in_e; nd.dbg_in_i[id] = in_i; }
-                if (pd->pn) spk = run_neuron(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, model, pd->flags,
-                                             v, g1, g2, fr, in_e, in_i, i_ext, f);
-                else spk = run_neuron(SharedParams{pd->p}, model, pd->flags, v, g1, g2, fr, in_e, in_i, i_ext, f);
-                st0[id] = v;
-                st1[id] = g1;
-                if (model != SZSNN_IZHIKEVICH) { st2[id] = g2; st3[id] = fr; }
-            } else if (model == SZSNN_POISSON) {
-                const float prob = pd->pn ? pd->pn[id - pd->begin] : pd->p[0];
-                spk = sz_poisson_fires(pd->seed, id - pd->begin, t, prob) || f;
-            } else if (model == SZSNN_CONST_RATE) {
-                if (pd->pn) spk = sz_const_rate(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, v, f);
-                else spk = sz_const_rate(SharedParams{pd->p}, v, f);
-                st0[id] = v;
-            }
+            if (nd.dbg_in_e) { nd.dbg_in_e[id] = a.in_e; nd.dbg_in_i[id] = a.in_i; }
+            if (pd->pn) spk = run_neuron(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, model, pd->flags,
+                                         a.v, a.g1, a.g2, a.fr, a.in_e, a.in_i, a.i_ext, a.f);
+            else spk = run_neuron(SharedParams{pd->p}, model, pd->flags, a.v, a.g1, a.g2, a.fr, a.in_e, a.in_i,
+                                  a.i_ext, a.f);
+            nd.st0[id] = a.v;
+            nd.st1[id] = a.g1;
+            if (model != SZSNN_IZHIKEVICH) { nd.st2[id] = a.g2; nd.st3[id] = a.fr; }
+        } else if (model == SZSNN_POISSON) {
+            const float prob = pd->pn ? pd->pn[id - pd->begin] : pd->p[0];
+            spk = sz_poisson_fires(pd->seed, id - pd->begin, t, prob) || a.f;
+        } else if (model == SZSNN_CONST_RATE) {
+            if (pd->pn) spk = sz_const_rate(UnitParams{pd->pn, id - pd->begin, pd->end - pd->begin}, a.v, a.f);
+            else spk = sz_const_rate(SharedParams{pd->p}, a.v, a.f);
+            nd.st0[id] = a.v;
         }
     }
-    // one call site for every lane: the epilogue's warp collectives are reached
-    // by the whole warp at the same instruction
-    __syncwarp();
-    update_spikes(nd, t, id, spk, lane, out_words);
+    return spk;
 }
 
-__global__ void __launch_bounds__(1024) k_update(NetDev nd, int k_off, const uint32_t* __restrict__ forced,
+// The loads of one unit (state, the inputs of step t from the parity buffer
+// the host names, forced spike, external current).
+__device__ __forceinline__ void load_unit(const NetDev& nd, const InBuf& inb, int64_t id,
+                                          const uint32_t* __restrict__ forced, const float* __restrict__ current,
+                                          UnitIn& a)
+{
+    a = UnitIn{};
+    if (id >= nd.U) return;
+    const uint32_t u = (uint32_t)id;
+    a.v = nd.st0[u];
+    if (id < nd.N) {
+        a.g1 = nd.st1[u];
+        a.g2 = nd.st2[u];
+        a.fr = nd.st3[u];
+        if (nd.acc_mode == SZSNN_ACC_FIXED) { a.fxe = inb.fe[u]; a.fxi = inb.fi[u]; }
+        else { a.in_e = inb.e[u]; a.in_i = inb.i[u]; }
+        if (current) a.i_ext = current[u];
+    }
+    if (forced) a.f = ((forced[u >> 5] >> (u & 31)) & 1u) != 0u;
+}
+
+// Block b covers units [b * T, (b + 1) * T), T = UPD_UPT * blockDim.x.  A
+// block the host marked as lying inside one population of the parameter
+// table runs an inline tile; other blocks run the generic update one
+// block-size sub-tile at a time (thread's unit j * blockDim.x + threadIdx.x),
+// each sub-tile ending in the spike epilogue, so every warp's units of a
+// sub-tile are 32 consecutive ids (one raster word).
+// Overlapped stepping: the warps with spikes deliver their units' m = 1
+// buckets into the buffer of t+1, and block 0 does the per-step bookkeeping.
+__device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk, const uint32_t* __restrict__ forced,
+                                            const float* __restrict__ current, uint32_t* __restrict__ out_words)
+{
+    extern __shared__ __align__(128) unsigned char upd_smem[];
+    const uint32_t bs = blockDim.x;
+    const int64_t tile0 = (int64_t)blk * UPD_UPT * bs;
+    const uint32_t lane = threadIdx.x & 31;
+    const long long t = *nd.clock + k_off;
+    const InBuf inb = in_buf_k(nd, k_off);
+    int slot = -1;
+#pragma unroll
+    for (int i = 0; i < INLINE_POPS; ++i)
+        if (blk >= nd.ib_lo[i] && blk < nd.ib_hi[i]) slot = i;
+    if (slot >= 0) {
+        if (nd.acc_mode == SZSNN_ACC_FIXED) tile_run_slot<true>(nd, slot, inb, tile0, t, forced, current, out_words, upd_smem);
+        else tile_run_slot<false>(nd, slot, inb, tile0, t, forced, current, out_words, upd_smem);
+    } else {
+        const StagedPops sp_ = stage_pops(nd, blk);
+#pragma unroll 1
+        for (int j = 0; j < UPD_UPT; ++j) {
+            const int64_t id = tile0 + (int64_t)j * bs + threadIdx.x;
+            UnitIn a;
+            load_unit(nd, inb, id, forced, current, a);
+            const bool spk = update_generic(nd, sp_, id, inb, t, a);
+            __syncwarp();
+            update_spikes(nd, t, id, spk, lane, out_words);
+        }
+    }
+    if (nd.overlap && blk == 0 && threadIdx.x == 0) {
+        step_bookkeeping(nd, t);
+        // the inputs were read by the launch's parity, the deliveries write by
+        // the step counter's: they must name the same buffer
+        if (((uint64_t)t ^ (uint64_t)(nd.par0 + (uint32_t)k_off)) & 1u)
+            dev_error(nd.err, SZSNN_DEV_STEP_PARITY, (uint32_t)t);
+    }
+}
+
+__global__ void __launch_bounds__(UPD_MAX_BLOCK) k_update(const __grid_constant__ NetDev nd, int k_off, const uint32_t* __restrict__ forced,
                                                 const float* __restrict__ current, uint32_t* __restrict__ out_words)
 {
     update_body(nd, k_off, blockIdx.x, forced, current, out_words);
@@ -591,7 +781,7 @@ __global__ void __launch_bounds__(1024) k_update(NetDev nd, int k_off, const uin
 // delivery blocks come first so they are resident from the start and run
 // beside the update blocks.
 template <int G>
-__global__ void __launch_bounds__(1024) k_step(NetDev nd, int k_off, int far_blocks, const uint32_t* __restrict__ forced,
+__global__ void __launch_bounds__(UPD_MAX_BLOCK) k_step(const __grid_constant__ NetDev nd, int k_off, int far_blocks, const uint32_t* __restrict__ forced,
                                               const float* __restrict__ current, uint32_t* __restrict__ out_words)
 {
     if ((int)blockIdx.x < far_blocks) {  // G > 0: grouped delivery, G lanes per bucket; G < 0: flattened, -G items per warp
@@ -730,6 +920,23 @@ NetDev make_dev(szsnn_net* n)
     d.dbg_in_e = nullptr; d.dbg_in_i = nullptr;
     d.group = n->d_group; d.group_spikes = n->d_group_spikes;
     d.blk_pop = n->d_blk_pop;
+    d.par0 = (uint32_t)(n->steps_done & 1);
+    // parameter-table slots: the populations with shared parameters and a model
+    // the inline update covers, each with the update blocks that lie inside it
+    if (n->npops <= INLINE_POPS) {
+        const int64_t bs = (int64_t)n->upd_block * UPD_UPT;  // units per update block
+        for (int i = 0; i < n->npops; ++i) {
+            const PopDev& q = n->h_pops[(size_t)i];
+            const bool ok = !q.pn && (q.model == SZSNN_IF_CURR_EXP || q.model == SZSNN_IF_COND_EXP ||
+                                      q.model == SZSNN_IZHIKEVICH || q.model == SZSNN_POISSON);
+            const int64_t lo = sz_div_up(q.begin, bs);                        // first block starting inside
+            const int64_t hi = q.end >= n->U ? sz_div_up(n->U, bs) : q.end / bs;  // blocks ending inside
+            if (!ok || hi <= lo) continue;
+            d.ipop[i] = q;
+            d.ib_lo[i] = (int32_t)lo;
+            d.ib_hi[i] = (int32_t)hi;
+        }
+    }
     return d;
 }
 
@@ -767,11 +974,11 @@ cudaError_t launch_propagate_far(szsnn_net* n, const NetDev& d, int k_off, cudaS
     return launch_propagate(n, d, k_off, 2, PF_PENDING, st);
 }
 
-// (first pop, count) overlapping each update block of `bs` threads
+// (first pop, count) overlapping the tile of each update block
 cudaError_t fill_blk_pop(szsnn_net* n)
 {
     if (n->npops <= UPD_BLOCK_POPS) return cudaSuccess;
-    const int bs = n->upd_block;
+    const int64_t bs = (int64_t)n->upd_block * UPD_UPT;  // units per update block (its tile)
     const int64_t nb = sz_div_up(n->U, bs);
     std::vector<int2> t((size_t)nb);
     int first = 0;
@@ -783,7 +990,7 @@ cudaError_t fill_blk_pop(szsnn_net* n)
         t[(size_t)b] = make_int2(first, c);
     }
     if (!n->d_blk_pop) {
-        cudaError_t e = cudaMalloc((void**)&n->d_blk_pop, (size_t)sz_div_up(n->U, 32) * sizeof(int2));
+        cudaError_t e = cudaMalloc((void**)&n->d_blk_pop, (size_t)sz_div_up(n->U, 32 * UPD_UPT) * sizeof(int2));
         if (e != cudaSuccess) return e;
     }
     cudaError_t e = cudaMemcpyAsync(n->d_blk_pop, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, n->ctx->stream);
@@ -791,12 +998,28 @@ cudaError_t fill_blk_pop(szsnn_net* n)
     return cudaStreamSynchronize(n->ctx->stream);
 }
 
+// dynamic shared memory of an update launch: an inline tile when any block
+// of the launch runs one; the kernel's limit raised when that is above 48 KB
+template <class K>
+cudaError_t update_smem(const NetDev& d, int bs, K kernel, size_t* bytes)
+{
+    bool any = false;
+    for (int i = 0; i < INLINE_POPS; ++i) any = any || d.ib_hi[i] > d.ib_lo[i];
+    *bytes = any ? tile_smem_bytes((int64_t)UPD_UPT * bs, d.acc_mode == SZSNN_ACC_FIXED) : 0;
+    if (*bytes > 48 * 1024)
+        return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*bytes);
+    return cudaSuccess;
+}
+
 cudaError_t launch_update(szsnn_net* n, const NetDev& d, int k_off, const uint32_t* forced, const float* cur,
                           uint32_t* words, cudaStream_t st)
 {
     int bs = n->upd_block;
-    int64_t blocks = sz_div_up(n->U, bs);
-    k_update<<<(unsigned)blocks, bs, 0, st>>>(d, k_off, forced, cur, words);
+    int64_t blocks = sz_div_up(n->U, (int64_t)bs * UPD_UPT);
+    size_t smem = 0;
+    cudaError_t e = update_smem(d, bs, k_update, &smem);
+    if (e != cudaSuccess) return e;
+    k_update<<<(unsigned)blocks, bs, smem, st>>>(d, k_off, forced, cur, words);
     return cudaGetLastError();
 }
 
@@ -806,22 +1029,31 @@ cudaError_t launch_step(szsnn_net* n, const NetDev& d, int k_off, const uint32_t
 {
     const int bs = n->upd_block;
     const int far = n->D < 2 ? 0 : (n->prop_blocks > 0 ? n->prop_blocks : num_sms(n->ctx) * std::max(1, 1024 / bs));
-    const int64_t blocks = far + sz_div_up(n->U, bs);
+    const int64_t blocks = far + sz_div_up(n->U, (int64_t)bs * UPD_UPT);
     const dim3 grid((unsigned)blocks);
+    size_t smem = 0;
+    cudaError_t e = cudaSuccess;
+#define SZ_STEP(G)                                                         \
+    do {                                                                  \
+        e = update_smem(d, bs, k_step<G>, &smem);                         \
+        if (e == cudaSuccess) k_step<G><<<grid, bs, smem, st>>>(d, k_off, far, forced, cur, words); \
+    } while (0)
     if (n->prop_mode == 1) {
         switch (n->prop_group) {
-        case 8: k_step<-8><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
-        case 16: k_step<-16><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
-        default: k_step<-32><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
+        case 8: SZ_STEP(-8); break;
+        case 16: SZ_STEP(-16); break;
+        default: SZ_STEP(-32); break;
         }
-        return cudaGetLastError();
+    } else {
+        switch (n->prop_group) {
+        case 4: SZ_STEP(4); break;
+        case 8: SZ_STEP(8); break;
+        case 32: SZ_STEP(32); break;
+        default: SZ_STEP(16); break;
+        }
     }
-    switch (n->prop_group) {
-    case 4: k_step<4><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
-    case 8: k_step<8><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
-    case 32: k_step<32><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
-    default: k_step<16><<<grid, bs, 0, st>>>(d, k_off, far, forced, cur, words); break;
-    }
+#undef SZ_STEP
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
@@ -829,7 +1061,8 @@ template <class T>
 cudaError_t dalloc(T** p, size_t count)
 {
     *p = nullptr;
-    if (!count) count = 1;
+    count = (count + 31) & ~(size_t)31;  // room for bulk copies rounded up to 16 bytes
+    if (!count) count = 32;
     return cudaMalloc((void**)p, count * sizeof(T));
 }
 
@@ -967,6 +1200,7 @@ extern "C" int szsnn_net_create(szsnn_ctx* ctx, const szsnn_net_desc* d, szsnn_n
                 off += tmp.size();
             }
         }
+        n->h_pops = hp;
         C(dalloc(&n->d_pops, hp.size()));
         C(cudaMemcpyAsync(n->d_pops, hp.data(), hp.size() * sizeof(PopDev), cudaMemcpyHostToDevice, st));
         C(cudaStreamSynchronize(st));
@@ -1159,7 +1393,7 @@ extern "C" int szsnn_net_step(szsnn_net* n, const uint32_t* forced_host, const f
 // delivery ran in the previous step's launch, or at priming).
 static int net_graph(szsnn_net* n, int len, int flags, int b, cudaGraphExec_t* out)
 {
-    auto key = std::make_tuple(len, flags, b);
+    auto key = std::make_tuple(len, flags, b, (int)(n->steps_done & 1));
     auto it = n->graphs.find(key);
     if (it != n->graphs.end()) { *out = it->second; return SZSNN_OK; }
     cudaStream_t st = n->ctx->stream;
@@ -1479,8 +1713,8 @@ extern "C" int szsnn_net_set_tuning(szsnn_net* n, int mode, int group, int block
         return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "grouped propagate: lanes per bucket must be 4, 8, 16 or 32");
     if (mode == 1 && group != 0 && group != 8 && group != 16 && group != 32)
         return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "flattened propagate: items per warp must be 8, 16 or 32");
-    if (upd_block != 0 && (upd_block < 32 || upd_block > 1024 || upd_block % 32))
-        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "update block must be a multiple of 32 in 32..1024");
+    if (upd_block != 0 && (upd_block < 32 || upd_block > UPD_MAX_BLOCK || upd_block % 32))
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "update block must be a multiple of 32 in 32..256");
     n->prop_mode = mode;
     n->prop_group = group ? group : (mode == 1 ? 32 : 16);
     if (blocks >= 0) n->prop_blocks = blocks;
@@ -1777,7 +2011,7 @@ extern "C" int szsnn_step_static(const szsnn_static_step* s, char* err, size_t e
     k_propagate<16><<<sms * 16, 256, 0, st>>>(d, 0, 1, PF_ZERO_SLOT | PF_SPIKES);
     e = cudaGetLastError();
     if (e == cudaSuccess) {
-        k_update<<<(unsigned)sz_div_up(U, 256), 256, 0, st>>>(d, 0, nullptr, nullptr, s->fired_words);
+        k_update<<<(unsigned)sz_div_up(U, 256 * UPD_UPT), 256, 0, st>>>(d, 0, nullptr, nullptr, s->fired_words);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess)

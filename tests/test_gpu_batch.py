@@ -71,7 +71,7 @@ def test_autotune_keeps_results(ctx, tmp_path, monkeypatch):
     ref.close()
     bt = B.Batch(ctx, specs, acc_mode=L.ACC_FIXED)
     choice = tune(bt.net, replays=5)
-    assert choice["update_block"] in (128, 256, 512) and not choice["cached"]
+    assert choice["update_block"] in (64, 128, 256) and not choice["cached"]
     assert tune(bt.net, replays=5)["cached"]  # same device, same workload shape
     # the tuning replays ran on scratch state: the simulation still starts at step 0
     assert bt.net.stats()["steps_done"] == 0
