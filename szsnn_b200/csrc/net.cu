@@ -39,8 +39,9 @@
 // (IF models), computed once on the host with the same fp32 operations
 #define POP_SLOTS 16
 #define INLINE_POPS 4
-#define UPD_UPT 4        // units per update thread, strided by the block size
+#define UPD_UPT 4        // most units per update thread (strided by the block size)
 #define UPD_MAX_BLOCK 256  // update threads per block (the step kernel's block too)
+#define UPD_MIN_BLOCKS 6   // resident blocks of UPD_MAX_BLOCK per SM the register budget keeps
 struct PopDev {
     int32_t model;
     uint32_t flags;
@@ -82,6 +83,7 @@ struct NetDev {
     unsigned long long* group_spikes;      // [n_groups]
     const int2* blk_pop;                   // per update block: (first overlapping pop, count)
     uint32_t par0;                         // parity of the step counter when the launch runs
+    int32_t upt;                           // units per update thread (1..UPD_UPT)
     int32_t ib_lo[INLINE_POPS], ib_hi[INLINE_POPS];  // update blocks [lo, hi) lying inside slot i (empty: none)
     PopDev ipop[INLINE_POPS];              // populations with shared parameters, by value in the kernel parameters
 };
@@ -444,7 +446,7 @@ struct UnitIn {
 
 // ---- inline tiles: blocks inside one population of the parameter table
 //
-// The block's tile of T = UPD_UPT * blockDim.x units is brought into shared
+// The block's tile of T = nd.upt * blockDim.x units is brought into shared
 // memory by bulk copies (one per state / input array, issued by one thread,
 // completing on an mbarrier), so the bytes in flight are bounded by shared
 // memory rather than by registers.  Each thread then updates units
@@ -577,18 +579,18 @@ __device__ __forceinline__ bool tile_unit(const NetDev& nd, const PopDev& P, con
 }
 
 // The whole inline tile with population slot PI and model MODEL: bulk load,
-// then the UPD_UPT sub-tiles, each ending in the spike epilogue.
+// then the nd.upt sub-tiles, each ending in the spike epilogue.
 template <int MODEL, bool FIXED, int PI>
 __device__ __forceinline__ void tile_run(const NetDev& nd, const InBuf& inb, int64_t tile0, long long t,
                                         const uint32_t* __restrict__ forced, const float* __restrict__ current,
                                         uint32_t* __restrict__ out_words, unsigned char* smem)
 {
-    const uint32_t bs = blockDim.x, T = UPD_UPT * bs, lane = threadIdx.x & 31;
+    const uint32_t bs = blockDim.x, T = (uint32_t)nd.upt * bs, lane = threadIdx.x & 31;
     const TileSmem sm = tile_smem(smem, T, FIXED);
     const bool ok = tile_load<MODEL, FIXED>(nd, inb, tile0, T, sm);
     const PopDev& P = nd.ipop[PI];
 #pragma unroll 1
-    for (int j = 0; j < UPD_UPT; ++j) {
+    for (int j = 0; j < nd.upt; ++j) {
         const uint32_t u = (uint32_t)j * bs + threadIdx.x;
         const int64_t id = tile0 + u;
         bool spk = false;
@@ -724,7 +726,7 @@ __device__ __forceinline__ void load_unit(const NetDev& nd, const InBuf& inb, in
     if (forced) a.f = ((forced[u >> 5] >> (u & 31)) & 1u) != 0u;
 }
 
-// Block b covers units [b * T, (b + 1) * T), T = UPD_UPT * blockDim.x.  A
+// Block b covers units [b * T, (b + 1) * T), T = nd.upt * blockDim.x.  A
 // block the host marked as lying inside one population of the parameter
 // table runs an inline tile; other blocks run the generic update one
 // block-size sub-tile at a time (thread's unit j * blockDim.x + threadIdx.x),
@@ -737,7 +739,7 @@ __device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk
 {
     extern __shared__ __align__(128) unsigned char upd_smem[];
     const uint32_t bs = blockDim.x;
-    const int64_t tile0 = (int64_t)blk * UPD_UPT * bs;
+    const int64_t tile0 = (int64_t)blk * nd.upt * bs;
     const uint32_t lane = threadIdx.x & 31;
     const long long t = *nd.clock + k_off;
     const InBuf inb = in_buf_k(nd, k_off);
@@ -751,7 +753,7 @@ __device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk
     } else {
         const StagedPops sp_ = stage_pops(nd, blk);
 #pragma unroll 1
-        for (int j = 0; j < UPD_UPT; ++j) {
+        for (int j = 0; j < nd.upt; ++j) {
             const int64_t id = tile0 + (int64_t)j * bs + threadIdx.x;
             UnitIn a;
             load_unit(nd, inb, id, forced, current, a);
@@ -769,7 +771,7 @@ __device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk
     }
 }
 
-__global__ void __launch_bounds__(UPD_MAX_BLOCK) k_update(const __grid_constant__ NetDev nd, int k_off, const uint32_t* __restrict__ forced,
+__global__ void __launch_bounds__(UPD_MAX_BLOCK, UPD_MIN_BLOCKS) k_update(const __grid_constant__ NetDev nd, int k_off, const uint32_t* __restrict__ forced,
                                                 const float* __restrict__ current, uint32_t* __restrict__ out_words)
 {
     update_body(nd, k_off, blockIdx.x, forced, current, out_words);
@@ -781,7 +783,7 @@ __global__ void __launch_bounds__(UPD_MAX_BLOCK) k_update(const __grid_constant_
 // delivery blocks come first so they are resident from the start and run
 // beside the update blocks.
 template <int G>
-__global__ void __launch_bounds__(UPD_MAX_BLOCK) k_step(const __grid_constant__ NetDev nd, int k_off, int far_blocks, const uint32_t* __restrict__ forced,
+__global__ void __launch_bounds__(UPD_MAX_BLOCK, UPD_MIN_BLOCKS) k_step(const __grid_constant__ NetDev nd, int k_off, int far_blocks, const uint32_t* __restrict__ forced,
                                               const float* __restrict__ current, uint32_t* __restrict__ out_words)
 {
     if ((int)blockIdx.x < far_blocks) {  // G > 0: grouped delivery, G lanes per bucket; G < 0: flattened, -G items per warp
@@ -906,6 +908,16 @@ __global__ void k_unpack_syn(const int2* syn, int32_t* tgt, float* w, uint64_t n
 
 int num_sms(szsnn_ctx* ctx) { return ctx->num_sms > 0 ? ctx->num_sms : 148; }
 
+// Units per update thread: UPD_UPT (bulk-copied tiles, fewer and longer
+// blocks) only while the update grid still holds at least four blocks per SM;
+// smaller networks keep one unit per thread, where the step is latency-bound
+// and more blocks in parallel shorten it.
+int upd_upt(const szsnn_net* n)
+{
+    const int64_t per_sm = sz_div_up(n->U, (int64_t)num_sms(n->ctx) * n->upd_block);  // blocks per SM at 1 unit
+    return (int)std::max<int64_t>(1, std::min<int64_t>(UPD_UPT, per_sm / 4));
+}
+
 NetDev make_dev(szsnn_net* n)
 {
     NetDev d{};
@@ -921,10 +933,11 @@ NetDev make_dev(szsnn_net* n)
     d.group = n->d_group; d.group_spikes = n->d_group_spikes;
     d.blk_pop = n->d_blk_pop;
     d.par0 = (uint32_t)(n->steps_done & 1);
+    d.upt = upd_upt(n);
     // parameter-table slots: the populations with shared parameters and a model
     // the inline update covers, each with the update blocks that lie inside it
     if (n->npops <= INLINE_POPS) {
-        const int64_t bs = (int64_t)n->upd_block * UPD_UPT;  // units per update block
+        const int64_t bs = (int64_t)n->upd_block * d.upt;  // units per update block
         for (int i = 0; i < n->npops; ++i) {
             const PopDev& q = n->h_pops[(size_t)i];
             const bool ok = !q.pn && (q.model == SZSNN_IF_CURR_EXP || q.model == SZSNN_IF_COND_EXP ||
@@ -978,7 +991,7 @@ cudaError_t launch_propagate_far(szsnn_net* n, const NetDev& d, int k_off, cudaS
 cudaError_t fill_blk_pop(szsnn_net* n)
 {
     if (n->npops <= UPD_BLOCK_POPS) return cudaSuccess;
-    const int64_t bs = (int64_t)n->upd_block * UPD_UPT;  // units per update block (its tile)
+    const int64_t bs = (int64_t)n->upd_block * upd_upt(n);  // units per update block (its tile)
     const int64_t nb = sz_div_up(n->U, bs);
     std::vector<int2> t((size_t)nb);
     int first = 0;
@@ -990,7 +1003,7 @@ cudaError_t fill_blk_pop(szsnn_net* n)
         t[(size_t)b] = make_int2(first, c);
     }
     if (!n->d_blk_pop) {
-        cudaError_t e = cudaMalloc((void**)&n->d_blk_pop, (size_t)sz_div_up(n->U, 32 * UPD_UPT) * sizeof(int2));
+        cudaError_t e = cudaMalloc((void**)&n->d_blk_pop, (size_t)sz_div_up(n->U, 32) * sizeof(int2));
         if (e != cudaSuccess) return e;
     }
     cudaError_t e = cudaMemcpyAsync(n->d_blk_pop, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, n->ctx->stream);
@@ -1005,7 +1018,7 @@ cudaError_t update_smem(const NetDev& d, int bs, K kernel, size_t* bytes)
 {
     bool any = false;
     for (int i = 0; i < INLINE_POPS; ++i) any = any || d.ib_hi[i] > d.ib_lo[i];
-    *bytes = any ? tile_smem_bytes((int64_t)UPD_UPT * bs, d.acc_mode == SZSNN_ACC_FIXED) : 0;
+    *bytes = any ? tile_smem_bytes((int64_t)d.upt * bs, d.acc_mode == SZSNN_ACC_FIXED) : 0;
     if (*bytes > 48 * 1024)
         return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*bytes);
     return cudaSuccess;
@@ -1015,7 +1028,7 @@ cudaError_t launch_update(szsnn_net* n, const NetDev& d, int k_off, const uint32
                           uint32_t* words, cudaStream_t st)
 {
     int bs = n->upd_block;
-    int64_t blocks = sz_div_up(n->U, (int64_t)bs * UPD_UPT);
+    int64_t blocks = sz_div_up(n->U, (int64_t)bs * d.upt);
     size_t smem = 0;
     cudaError_t e = update_smem(d, bs, k_update, &smem);
     if (e != cudaSuccess) return e;
@@ -1029,7 +1042,7 @@ cudaError_t launch_step(szsnn_net* n, const NetDev& d, int k_off, const uint32_t
 {
     const int bs = n->upd_block;
     const int far = n->D < 2 ? 0 : (n->prop_blocks > 0 ? n->prop_blocks : num_sms(n->ctx) * std::max(1, 1024 / bs));
-    const int64_t blocks = far + sz_div_up(n->U, (int64_t)bs * UPD_UPT);
+    const int64_t blocks = far + sz_div_up(n->U, (int64_t)bs * d.upt);
     const dim3 grid((unsigned)blocks);
     size_t smem = 0;
     cudaError_t e = cudaSuccess;
@@ -2008,10 +2021,11 @@ extern "C" int szsnn_step_static(const szsnn_static_step* s, char* err, size_t e
     d.clock = (const long long*)base;
     d.stats = (unsigned long long*)(base + 64);
     d.err = s->error_word ? s->error_word : (uint32_t*)(base + 128);
+    d.upt = 1;
     k_propagate<16><<<sms * 16, 256, 0, st>>>(d, 0, 1, PF_ZERO_SLOT | PF_SPIKES);
     e = cudaGetLastError();
     if (e == cudaSuccess) {
-        k_update<<<(unsigned)sz_div_up(U, 256 * UPD_UPT), 256, 0, st>>>(d, 0, nullptr, nullptr, s->fired_words);
+        k_update<<<(unsigned)sz_div_up(U, 256), 256, 0, st>>>(d, 0, nullptr, nullptr, s->fired_words);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess)
