@@ -389,6 +389,11 @@ def main():
     e2e_steps = min(args.e2e_steps, args.steps)
     forced, raster = pinned_words(e2e_steps, net.words), pinned_words(e2e_steps, net.words)
     forced[:] = 0
+    # untimed warm-up through the same call: the graphs of host-I/O chunks (both
+    # stage buffers) are captured and instantiated once, outside the timed run
+    warm = min(e2e_steps, 2 * net.graph_chunk)
+    net.run(warm, forced_words=forced[:warm], out=raster[:warm])
+    ctx.sync()
     s2 = net.stats()
     barrier()
     t_e2e = time.perf_counter()

@@ -121,7 +121,8 @@ struct szsnn_net {
     float* d_dbg_in = nullptr;
     uint32_t* h_pinned_words = nullptr;  // pinned: one step's words (szsnn_net_step)
     uint32_t* h_io[4] = {};              // pinned bounce buffers for pageable host arrays: in0, in1, out0, out1
-    cudaStream_t copy_st = nullptr;      // host <-> device copies of szsnn_net_run
+    cudaStream_t copy_st = nullptr;      // host -> device copies of szsnn_net_run (forced words)
+    cudaStream_t copy_out_st = nullptr;  // device -> host copies of szsnn_net_run (raster)
     cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {};
     bool overlap = true;
     std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;  // (steps, io flags, stage, step parity)
@@ -1113,6 +1114,7 @@ void free_net(szsnn_net* n)
     for (int p = 0; p < 2; ++p)
         for (cudaEvent_t ev : {n->ev_in[p], n->ev_comp[p], n->ev_out[p]}) if (ev) cudaEventDestroy(ev);
     if (n->copy_st) cudaStreamDestroy(n->copy_st);
+    if (n->copy_out_st) cudaStreamDestroy(n->copy_out_st);
     delete n;
 }
 
@@ -1285,6 +1287,7 @@ extern "C" int szsnn_net_create(szsnn_ctx* ctx, const szsnn_net_desc* d, szsnn_n
     C(cudaEventCreate(&n->ev_run0));
     C(cudaEventCreate(&n->ev_run1));
     C(cudaStreamCreateWithFlags(&n->copy_st, cudaStreamNonBlocking));
+    C(cudaStreamCreateWithFlags(&n->copy_out_st, cudaStreamNonBlocking));
     for (int p = 0; p < 2; ++p) {
         C(cudaEventCreateWithFlags(&n->ev_in[p], cudaEventDisableTiming));
         C(cudaEventCreateWithFlags(&n->ev_comp[p], cudaEventDisableTiming));
@@ -1490,8 +1493,9 @@ static bool host_pinned(const void* p, size_t bytes)
 }
 
 // Chunks of `chunk` steps, each one graph launch.  Host / device copies of the
-// forced words and the raster run on the copy stream into alternating stage
-// buffers, so chunk k's copies overlap chunk k-1's / k+1's compute.  Pinned
+// forced words and of the raster run on two copy streams (one per direction)
+// into alternating stage buffers, so chunk k+1's input copy and chunk k-1's
+// raster copy both overlap chunk k's compute.  Pinned
 // host arrays are copied directly; pageable ones go through pinned bounce
 // buffers (the copy-out of chunk k to the caller's array happens while chunk
 // k+1 runs).
@@ -1499,7 +1503,7 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
                         bool host)
 {
     if (!n || steps < 0) return SZSNN_ERR_ARG;
-    cudaStream_t st = n->ctx->stream, cp = n->copy_st;
+    cudaStream_t st = n->ctx->stream, cp = n->copy_st, cpo = n->copy_out_st;
     const size_t wbytes = (size_t)n->words * 4;
     const bool pin_in = host && forced && host_pinned(forced, (size_t)steps * wbytes);
     const bool pin_out = host && raster && host_pinned(raster, (size_t)steps * wbytes);
@@ -1510,6 +1514,7 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
     }
     NET_TRY(n, cudaEventRecord(n->ev_run0, st));
     NET_TRY(n, cudaStreamWaitEvent(cp, n->ev_run0, 0));  // copies follow earlier work on the main stream
+    NET_TRY(n, cudaStreamWaitEvent(cpo, n->ev_run0, 0));
     const cudaMemcpyKind in_kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     const cudaMemcpyKind out_kind = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     struct Pending { bool on; size_t off, bytes; };
@@ -1552,10 +1557,10 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
         if (raster) {
             rc = flush(b);  // bounce b last held chunk k-2
             if (rc) return rc;
-            NET_TRY(n, cudaStreamWaitEvent(cp, n->ev_comp[b], 0));
+            NET_TRY(n, cudaStreamWaitEvent(cpo, n->ev_comp[b], 0));
             char* dst = bounce_out ? (char*)n->h_io[2 + b] : (char*)raster + off;
-            NET_TRY(n, cudaMemcpyAsync(dst, n->d_raster_stage[b], bytes, out_kind, cp));
-            NET_TRY(n, cudaEventRecord(n->ev_out[b], cp));
+            NET_TRY(n, cudaMemcpyAsync(dst, n->d_raster_stage[b], bytes, out_kind, cpo));
+            NET_TRY(n, cudaEventRecord(n->ev_out[b], cpo));
             if (bounce_out) pend[b] = Pending{true, off, bytes};
             rc = flush(b ^ 1);  // chunk k-1, copied while chunk k computes
             if (rc) return rc;
@@ -1567,9 +1572,11 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
         int rc = flush(b);
         if (rc) return rc;
     }
-    // the main stream resumes after the last copies
+    // the main stream resumes after the last copies of both directions
     NET_TRY(n, cudaEventRecord(n->ev_in[0], cp));
     NET_TRY(n, cudaStreamWaitEvent(st, n->ev_in[0], 0));
+    NET_TRY(n, cudaEventRecord(n->ev_out[0], cpo));
+    NET_TRY(n, cudaStreamWaitEvent(st, n->ev_out[0], 0));
     NET_TRY(n, cudaEventRecord(n->ev_run1, st));
     n->run_timed = true;
     if (host) NET_TRY(n, cudaStreamSynchronize(st));  // host arrays are complete on return

@@ -131,6 +131,9 @@ class Network:
         L.check(self.lib.szsnn_net_create(ctx.h, C.byref(d), C.byref(h)), ctx.h, "net_create")
         self.h = h.value
         self.n_synapses = int(d.n_synapses)
+        self.graph_chunk = graph_chunk  # steps per CUDA graph (0: the library's default of 100)
+        if not self.graph_chunk:
+            self.graph_chunk = 100
 
     def generate(self, blocks: list[GenBlock], seed: int) -> None:
         off = 0
