@@ -9,7 +9,10 @@
     state and event counts;
   * host arrays in page-locked memory (DMA) and pageable memory (bounce
     buffers), and device arrays, give the same raster, for chunk counts that
-    exercise both stage buffers.
+    exercise both stage buffers;
+  * the update's tiles of four units per thread (bulk-copied inline tiles for
+    IF_cond_exp, IF_curr_exp, Izhikevich and Poisson, and a generic tile across
+    a population boundary) equal the oracle in both step orders.
 """
 import numpy as np
 import pytest
@@ -142,3 +145,64 @@ def test_host_io_pinned_pageable_and_device(ctx):
     assert int(np.unpackbits(r_page.view(np.uint8)).sum()) > 1000
     for net in nets:
         net.close()
+
+
+# Tiles of four units per thread.  The update picks them when its grid still
+# holds at least four blocks per SM; with 32-thread update blocks that is from
+# 75,776 units on (110,000 units: ceil(110000 / (148 * 32)) = 24 blocks per SM
+# at one unit per thread, 24 / 4 >= 4).  Each tile of 128 units inside one
+# population is brought into shared memory by bulk copies; the tile that
+# straddles the neuron / source boundary runs the generic update.
+TILE_N, TILE_P = 100_000, 10_000
+
+
+@pytest.mark.parametrize("overlap", [True, False])
+def test_four_unit_tiles_cond_equal_oracle(ctx, overlap):
+    n, p, D = TILE_N, TILE_P, 16
+    blocks, pops, st = cond_network(n, p, fanout=40, D=D, seed=8)
+    net = sz.Network(ctx, n, p, D, pops, state=st, acc_mode=L.ACC_FIXED, graph_chunk=25)
+    net.generate(blocks, seed=77)
+    net.set_overlap(overlap)
+    net.set_tuning(1, 32, 0, 32)
+    on = oracle.OracleNet(n, p, D, pops, oracle.generate(blocks, 77, n + p, D), state=st)
+    r = net.run(60)
+    ro, ev = on.run(60, acc_mode=oracle.ACC_FIXED)
+    assert int(np.unpackbits(ro.view(np.uint8)).sum()) > 1000
+    assert np.array_equal(r, ro)
+    for k in range(4):
+        assert np.array_equal(net.get_state(k), on.state[k])
+    assert net.stats()["events"] == ev
+    net.close()
+
+
+def _forced_tile_net(ctx, model, overlap):
+    n = TILE_N + TILE_P
+    net_ = if_network(n=n, n_syn=40 * n, max_delay=8, dyadic=False, seed=12)
+    csr = sz.csr_from_synapses(n, 8, net_["src"], net_["tgt"], net_["w"], net_["d1"])
+    if model == sz.IZHIKEVICH:
+        pv = np.zeros(12, np.float32)
+        pv[:4] = (0.02, 0.2, -65.0, 8.0)
+        v0 = np.full(n, -65.0, np.float32) + net_["v0"] + 60.0
+        st = [v0, (0.2 * v0).astype(np.float32), None, None]
+    else:
+        pv = net_["pv"]
+        st = [net_["v0"], None, None, np.full(n, 1e4, np.float32)]
+    pops = [sz.Pop(model, 0, n, pv)]
+    net = sz.Network(ctx, n, 0, 8, pops, csr=csr, state=st, acc_mode=L.ACC_FIXED, graph_chunk=25)
+    net.set_overlap(overlap)
+    net.set_tuning(1, 32, 0, 32)
+    return net, oracle.OracleNet(n, 0, 8, pops, csr, state=st), n
+
+
+@pytest.mark.parametrize("model,overlap", [(sz.IF_CURR_EXP, True), (sz.IZHIKEVICH, False)])
+def test_four_unit_tiles_forced_equal_oracle(ctx, model, overlap):
+    net, on, n = _forced_tile_net(ctx, model, overlap)
+    fw = forced_words(forced_schedule(n, 40), n)
+    r = net.run(40, forced_words=fw)
+    ro, ev = on.run(40, forced_words=fw, acc_mode=oracle.ACC_FIXED)
+    assert int(np.unpackbits(ro.view(np.uint8)).sum()) > 1000
+    assert np.array_equal(r, ro)
+    for k in range(2 if model == sz.IZHIKEVICH else 4):
+        assert np.array_equal(net.get_state(k), on.state[k])
+    assert net.stats()["events"] == ev
+    net.close()
