@@ -157,9 +157,17 @@ extern "C" int szsnn_sync(szsnn_ctx* ctx)
     uint32_t code = 0, info = 0;
     int rc = szsnn_device_error(ctx, &code, &info);
     if (rc) return rc;
-    if (code)
+    if (code) {
+        static const char* const names[] = {"", "synapse target outside the network", "queue slot full",
+                                            "spike ring slot full", "NaN or Inf in the state",
+                                            "delay outside 1..max_delay",
+                                            "launch parity disagrees with the step counter",
+                                            "a bounded bulk-copy wait ran out"};
+        const std::string what = code < sizeof(names) / sizeof(names[0]) ? names[code] : "unknown check";
         return szsnn_set_error(ctx, SZSNN_ERR_DEVICE,
-                               "device check failed: code " + std::to_string(code) + " info " + std::to_string(info));
+                               "device check failed: code " + std::to_string(code) + " (" + what + ") info " +
+                                   std::to_string(info));
+    }
     return SZSNN_OK;
 }
 

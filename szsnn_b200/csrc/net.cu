@@ -294,11 +294,11 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ NetDe
 // work item to its bucket segment; the warp then walks the concatenation of
 // those segments 32 synapses at a time (owner segment found by a binary
 // search over the lanes' exclusive offsets with shuffles), UNR loads in
-// flight per lane before their atomics.
-template <int IPW>
+// flight per lane before their atomics (8 in the delivery kernel of its own,
+// 4 inside the step kernel, whose register budget is shared with the update).
+template <int IPW, int UNR>
 __device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int m_lo, uint32_t pf, int blk, int nblk)
 {
-    constexpr int UNR = 4;
     __shared__ uint32_t s_pre[1025];
     __shared__ unsigned long long s_ev;
     const long long t = *nd.clock + k_off;
@@ -364,7 +364,7 @@ __device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int 
 template <int IPW>
 __global__ void __launch_bounds__(256) k_propagate_flat(const __grid_constant__ NetDev nd, int k_off, int m_lo, uint32_t pf)
 {
-    propagate_flat<IPW>(nd, k_off, m_lo, pf, blockIdx.x, gridDim.x);
+    propagate_flat<IPW, 8>(nd, k_off, m_lo, pf, blockIdx.x, gridDim.x);
 }
 
 // last population with begin <= id, or -1 (ranges sorted and disjoint)
@@ -403,18 +403,48 @@ __device__ __forceinline__ void update_spikes(const NetDev& nd, long long t, int
             else dev_error(nd.err, SZSNN_DEV_RING_OVERFLOW, (uint32_t)slot);
         }
         if (nd.overlap) {  // m = 1 buckets of this warp's spiking units into step t+1's inputs
+            // one walk over the concatenated buckets, 32 synapses per pass (owner
+            // lane by a search over the exclusive offsets), NEAR_UNR loads in
+            // flight per lane, so a warp of many spiking units pays a few round
+            // trips rather than one per unit
+            constexpr int NEAR_UNR = 2;
             const InBuf nb = in_buf(nd, t + 1);
             unsigned long long ra = 0, re = 0;
             if (spk) {
                 ra = nd.row_ptr[id * nd.D];
                 re = nd.row_ptr[id * nd.D + 1];
             }
+            const uint32_t len = (uint32_t)(re - ra);
+            uint32_t incl = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (uint32_t)o) incl += y;
+            }
+            const uint32_t excl = incl - len;
+            const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
             uint32_t ev = 0;
-            for (uint32_t bits = ball; bits; bits &= bits - 1u) {
-                const int l = __ffs(bits) - 1;
-                const unsigned long long a = __shfl_sync(0xffffffffu, ra, l);
-                const unsigned long long e = __shfl_sync(0xffffffffu, re, l);
-                for (unsigned long long q = a + lane; q < e; q += 32) deliver(nd, nb, nd.syn[q], ev);
+            for (uint32_t k0 = 0; k0 < tot; k0 += 32 * NEAR_UNR) {
+                int2 sw[NEAR_UNR];
+                bool ok[NEAR_UNR];
+#pragma unroll
+                for (int u = 0; u < NEAR_UNR; ++u) {
+                    const uint32_t k = k0 + 32u * u + lane;
+                    ok[u] = k < tot;
+                    int owner = 0;  // last lane whose segment starts at or before k
+#pragma unroll
+                    for (int st = 16; st >= 1; st >>= 1) {
+                        const int cand = owner + st;
+                        const uint32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
+                        if (cand < 32 && ex <= k) owner = cand;
+                    }
+                    const unsigned long long oa = __shfl_sync(0xffffffffu, ra, owner);
+                    const uint32_t oex = __shfl_sync(0xffffffffu, excl, owner);
+                    sw[u] = ok[u] ? nd.syn[oa + (k - oex)] : make_int2(0, 0);
+                }
+#pragma unroll
+                for (int u = 0; u < NEAR_UNR; ++u)
+                    if (ok[u]) deliver(nd, nb, sw[u], ev);
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
@@ -789,7 +819,7 @@ __global__ void __launch_bounds__(UPD_MAX_BLOCK, UPD_MIN_BLOCKS) k_step(const __
 {
     if ((int)blockIdx.x < far_blocks) {  // G > 0: grouped delivery, G lanes per bucket; G < 0: flattened, -G items per warp
         if constexpr (G > 0) propagate_grouped<G>(nd, k_off + 1, 2, PF_PENDING, blockIdx.x, far_blocks);
-        else propagate_flat<-G>(nd, k_off + 1, 2, PF_PENDING, blockIdx.x, far_blocks);
+        else propagate_flat<-G, 4>(nd, k_off + 1, 2, PF_PENDING, blockIdx.x, far_blocks);
         return;
     }
     update_body(nd, k_off, blockIdx.x - far_blocks, forced, current, out_words);
