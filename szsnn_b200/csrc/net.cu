@@ -56,6 +56,7 @@ struct NetDev {
     int32_t D, npops;
     const PopDev* pops;
     const unsigned long long* row_ptr;
+    const unsigned long long* rp_dm;  // delay-major copy: rp_dm[m * U + u] = row_ptr[u * D + m], m = 0..D; or null
     const int2* syn;
     float* st0;
     float* st1;
@@ -104,6 +105,7 @@ struct szsnn_net {
     int2* d_blk_pop = nullptr;             // per update-block tile: sized for 32-thread blocks, filled for upd_block
     uint64_t n_syn = 0;
     unsigned long long* d_row_ptr = nullptr;
+    unsigned long long* d_rp_dm = nullptr;     // delay-major copy of the bucket starts (delivery reads)
     int2* d_syn = nullptr;
     float* d_st[4] = {};
     float* d_in_e[2] = {};       // exc / inh inputs, one buffer per step parity (overlapped stepping)
@@ -183,6 +185,22 @@ __device__ __forceinline__ InBuf in_buf(const NetDev& nd, long long t)
 __device__ __forceinline__ InBuf in_buf_k(const NetDev& nd, int k_off)
 {
     return in_buf(nd, (long long)((nd.par0 + (uint32_t)k_off) & 1u));
+}
+
+// bounds [a, e) of bucket m (delay m, 1-based) of unit u, from the
+// delay-major copy (dm: warp-uniform; the warp's units are mostly consecutive,
+// so their bucket starts share sectors there) or from the unit-major row_ptr
+// (scattered units: both bounds of a bucket in one sector)
+__device__ __forceinline__ void bucket_bounds(const NetDev& nd, bool dm, int64_t u, int m, unsigned long long& a,
+                                              unsigned long long& e)
+{
+    if (dm) {
+        a = __ldg(&nd.rp_dm[(int64_t)(m - 1) * nd.U + u]);
+        e = __ldg(&nd.rp_dm[(int64_t)m * nd.U + u]);
+    } else {
+        a = __ldg(&nd.row_ptr[u * nd.D + (m - 1)]);
+        e = __ldg(&nd.row_ptr[u * nd.D + m]);
+    }
 }
 
 // one synapse into the exc / inh input of its target (weight sign picks the
@@ -277,8 +295,8 @@ __device__ __forceinline__ void propagate_grouped(const NetDev& nd, int k_off, i
         const uint32_t j = (uint32_t)(item - s_pre[m - 1]);
         const int64_t slot = (t - m) % R;
         const int64_t s = nd.ring_ids[slot * nd.U + j];
-        const unsigned long long a = nd.row_ptr[s * D + (m - 1)];
-        const unsigned long long e = nd.row_ptr[s * D + m];
+        unsigned long long a, e;
+        bucket_bounds(nd, false, s, m, a, e);
         for (unsigned long long q = a + lg; q < e; q += G) deliver(nd, buf, nd.syn[q], ev);
     }
     propagate_epilogue(nd, t, pf, ev, &s_ev);
@@ -314,6 +332,8 @@ __device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int 
     for (int64_t base = gw * IPW; base < (int64_t)total; base += nw * IPW) {
         const int64_t item = base + lane;
         unsigned long long a = 0, e = 0;
+        int64_t s = -1;
+        int mm = 0;  // the item's delay, 0 for lanes without one
         if (lane < (uint32_t)IPW && item < (int64_t)total) {
             int lo = 1, hi = D;
             while (lo < hi) {
@@ -322,10 +342,16 @@ __device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int 
             }
             const int m = lo;
             const uint32_t j = (uint32_t)(item - s_pre[m - 1]);
-            const int64_t s = __ldg(&nd.ring_ids[((t - m) % R) * nd.U + j]);
-            a = __ldg(&nd.row_ptr[s * D + (m - 1)]);
-            e = __ldg(&nd.row_ptr[s * D + m]);
+            s = __ldg(&nd.ring_ids[((t - m) % R) * nd.U + j]);
+            mm = m;
         }
+        // the delay-major index when most of the warp's items are consecutive
+        // units at one delay (a ring slot of a warp-wide burst), else row_ptr
+        const int64_t s_prev = __shfl_up_sync(0xffffffffu, s, 1);
+        const int m_prev = __shfl_up_sync(0xffffffffu, mm, 1);
+        const bool consec = lane > 0 && mm > 0 && m_prev == mm && s == s_prev + 1;
+        const bool dm = nd.rp_dm && __popc(__ballot_sync(0xffffffffu, consec)) >= IPW / 2;
+        if (mm > 0) bucket_bounds(nd, dm, s, mm, a, e);
         const uint32_t len = (uint32_t)(e - a);
         uint32_t incl = len;
 #pragma unroll
@@ -411,8 +437,7 @@ __device__ __forceinline__ void update_spikes(const NetDev& nd, long long t, int
             const InBuf nb = in_buf(nd, t + 1);
             unsigned long long ra = 0, re = 0;
             if (spk) {
-                ra = nd.row_ptr[id * nd.D];
-                re = nd.row_ptr[id * nd.D + 1];
+                bucket_bounds(nd, nd.rp_dm && __popc(ball) >= 8, id, 1, ra, re);
             }
             const uint32_t len = (uint32_t)(re - ra);
             uint32_t incl = len;
@@ -909,6 +934,18 @@ __global__ void __launch_bounds__(256) k_generate(GenDev g, int D, unsigned long
     }
 }
 
+// rp_dm[m * U + u] = row_ptr[u * D + m] for m = 0..D (row_ptr has U * D + 1
+// entries: m = D of unit u is the start of unit u+1, or the total)
+__global__ void k_rp_transpose(const unsigned long long* __restrict__ row_ptr, int64_t U, int D,
+                               unsigned long long* __restrict__ rp_dm)
+{
+    const int64_t n = (int64_t)(D + 1) * U;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t m = i / U, u = i - m * U;
+        rp_dm[i] = row_ptr[u * D + m];
+    }
+}
+
 __global__ void k_fill_rows(unsigned long long* row_ptr, int64_t s0, int64_t s1, int D, unsigned long long v)
 {
     for (int64_t i = s0 * D + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s1 * D;
@@ -953,7 +990,7 @@ NetDev make_dev(szsnn_net* n)
 {
     NetDev d{};
     d.N = n->N; d.U = n->U; d.words = n->words; d.D = n->D; d.npops = n->npops;
-    d.pops = n->d_pops; d.row_ptr = n->d_row_ptr; d.syn = n->d_syn;
+    d.pops = n->d_pops; d.row_ptr = n->d_row_ptr; d.rp_dm = n->d_rp_dm; d.syn = n->d_syn;
     d.st0 = n->d_st[0]; d.st1 = n->d_st[1]; d.st2 = n->d_st[2]; d.st3 = n->d_st[3];
     d.in_e = n->d_in_e[0]; d.in_i = n->d_in_i[0]; d.fx_e = n->d_fx_e[0]; d.fx_i = n->d_fx_i[0];
     d.in_e1 = n->d_in_e[1]; d.in_i1 = n->d_in_i[1]; d.fx_e1 = n->d_fx_e[1]; d.fx_i1 = n->d_fx_i[1];
@@ -1121,6 +1158,7 @@ void free_net(szsnn_net* n)
     cudaFree(n->d_group_spikes);
     cudaFree(n->d_blk_pop);
     cudaFree(n->d_row_ptr);
+    cudaFree(n->d_rp_dm);
     cudaFree(n->d_syn);
     for (int k = 0; k < 4; ++k) cudaFree(n->d_st[k]);
     for (int p = 0; p < 2; ++p) {
@@ -1158,6 +1196,18 @@ void free_net(szsnn_net* n)
                                                                             : SZSNN_ERR_CUDA,   \
                                    std::string(#call) + ": " + cudaGetErrorString(e_));         \
     } while (0)
+
+// the delay-major copy of row_ptr, rebuilt whenever the synapses change
+static cudaError_t build_rp_dm(szsnn_net* n)
+{
+    cudaStream_t st = n->ctx->stream;
+    if (!n->d_rp_dm) {
+        cudaError_t e = dalloc(&n->d_rp_dm, (size_t)(n->D + 1) * (size_t)n->U);
+        if (e != cudaSuccess) return e;
+    }
+    k_rp_transpose<<<num_sms(n->ctx) * 8, 256, 0, st>>>(n->d_row_ptr, n->U, n->D, n->d_rp_dm);
+    return cudaGetLastError();
+}
 
 extern "C" int szsnn_net_create(szsnn_ctx* ctx, const szsnn_net_desc* d, szsnn_net** out)
 {
@@ -1288,6 +1338,7 @@ extern "C" int szsnn_net_create(szsnn_ctx* ctx, const szsnn_net_desc* d, szsnn_n
     } else {
         C(cudaMemsetAsync(n->d_row_ptr, 0, ((size_t)U * D + 1) * 8, st));
     }
+    C(build_rp_dm(n));
     // state
     for (int k = 0; k < 4; ++k) {
         C(dalloc(&n->d_st[k], (size_t)U));
@@ -1389,6 +1440,7 @@ extern "C" int szsnn_net_generate(szsnn_net* n, const szsnn_gen_block* blocks, i
         }
         off += (uint64_t)b.src_count * (uint64_t)b.fanout;
     }
+    NET_TRY(n, build_rp_dm(n));
     NET_TRY(n, cudaStreamSynchronize(st));
     return SZSNN_OK;
 }
