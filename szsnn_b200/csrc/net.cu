@@ -1608,10 +1608,20 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
         pend[b].on = false;
         return SZSNN_OK;
     };
+    // Host runs with copies: a short first chunk (its input copy cannot overlap
+    // compute) and a short last chunk (nor can its raster copy), chunk / 8
+    // steps each, so the pipeline fills and drains quickly.
+    const bool edges = host && (forced || raster) && steps >= 2 * (int64_t)n->chunk;
+    const int64_t edge = std::max<int64_t>(1, n->chunk / 8);
     int64_t k = 0;
     for (int64_t done = 0; done < steps; ++k) {
         const int b = (int)(k & 1);
-        const int len = (int)std::min<int64_t>(n->chunk, steps - done);
+        const int64_t left = steps - done;
+        int len = (int)std::min<int64_t>(n->chunk, left);
+        if (edges) {
+            if (k == 0 || left <= edge) len = (int)std::min<int64_t>(edge, left);
+            else if (left < n->chunk + edge) len = (int)(left - edge);
+        }
         const int flags = (forced ? 1 : 0) | (current ? 2 : 0) | (raster ? 4 : 0);
         const size_t bytes = (size_t)len * wbytes, off = (size_t)done * wbytes;
         if (forced) {
