@@ -299,6 +299,20 @@ int szsnn_net_group_spikes(szsnn_net* net, uint64_t* counts, int reset);
 /* state slot k (length N+P) copy out / in (checkpoint) */
 int szsnn_net_get_state(szsnn_net* net, int slot, float* host);
 int szsnn_net_set_state(szsnn_net* net, int slot, const float* host);
+/* State monitor (no counterpart in the reference, whose print_vars.py reads the
+ * whole state back every cycle): after every step of szsnn_net_step / run /
+ * run_device, the state slots in slot_mask (bit k: slot k, 1..15) of the n_ids
+ * units ids[] are appended on the device to a trace of `capacity` steps; steps
+ * past the capacity are not recorded.  n_ids = 0 turns the monitor off.
+ * Recording starts at the current step; one extra small kernel per step. */
+int szsnn_net_set_monitor(szsnn_net* net, const int32_t* ids, int32_t n_ids, uint32_t slot_mask, int64_t capacity);
+/* The trace since szsnn_net_set_monitor or the last read: out [steps][slots][n_ids]
+ * fp32, slots in ascending order, at most max_steps; *steps_out = steps copied,
+ * *dropped_out = steps run since the start that were not copied (past the
+ * capacity or past max_steps).  Waits for the stream; recording then restarts
+ * at the current step. */
+int szsnn_net_monitor_read(szsnn_net* net, float* out, int64_t max_steps, int64_t* steps_out,
+                           int64_t* dropped_out);
 /* whole-simulation checkpoint: state, spike ring and clock into one blob */
 int szsnn_net_checkpoint_size(szsnn_net* net, uint64_t* bytes);
 int szsnn_net_checkpoint(szsnn_net* net, void* host_blob, uint64_t bytes);

@@ -119,6 +119,8 @@ SIGNATURES = {
     "szsnn_net_group_spikes": (_I, [_P, _P, _I]),
     "szsnn_net_get_state": (_I, [_P, _I, _P]),
     "szsnn_net_set_state": (_I, [_P, _I, _P]),
+    "szsnn_net_set_monitor": (_I, [_P, _P, C.c_int32, _U32, _I64]),
+    "szsnn_net_monitor_read": (_I, [_P, _P, _I64, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "szsnn_net_checkpoint_size": (_I, [_P, C.POINTER(C.c_uint64)]),
     "szsnn_net_checkpoint": (_I, [_P, _P, _U64]),
     "szsnn_net_restore": (_I, [_P, _P, _U64]),

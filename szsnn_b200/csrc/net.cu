@@ -102,6 +102,13 @@ struct szsnn_net {
     int32_t* d_group = nullptr;
     unsigned long long* d_group_spikes = nullptr;
     int32_t n_groups = 0;
+    // state monitor: recorded slots of chosen units, appended on the device after every step
+    int32_t* d_mon_ids = nullptr;
+    int32_t mon_n = 0;                     // monitored units (0: off)
+    uint32_t mon_slots = 0;                // bit k: state slot k recorded
+    float* d_mon_buf = nullptr;            // [capacity][slots][units]
+    long long* d_mon_t0 = nullptr;         // the step the trace starts at (device copy)
+    int64_t mon_cap = 0, mon_t0 = 0;
     int2* d_blk_pop = nullptr;             // per update-block tile: sized for 32-thread blocks, filled for upd_block
     uint64_t n_syn = 0;
     unsigned long long* d_row_ptr = nullptr;
@@ -161,6 +168,27 @@ __device__ __forceinline__ bool run_neuron(const P& p, int model, uint32_t flags
 }
 
 __global__ void k_advance(long long* clock, int k) { *clock += k; }
+
+// State monitor: after step t (= step counter + k_off) the recorded slots of
+// the monitored units go to row t - t0 of the trace, when it fits.
+__global__ void k_monitor(const long long* __restrict__ clock, int k_off, const long long* __restrict__ t0,
+                          const float* __restrict__ st0, const float* __restrict__ st1,
+                          const float* __restrict__ st2, const float* __restrict__ st3,
+                          const int32_t* __restrict__ ids, int n, uint32_t slots, float* __restrict__ buf,
+                          long long cap)
+{
+    const long long r = *clock + k_off - *t0;
+    if (r < 0 || r >= cap) return;
+    const int ns = __popc(slots);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t u = ids[i];
+        int j = 0;
+        if (slots & 1u) buf[((size_t)r * ns + j++) * n + i] = st0[u];
+        if (slots & 2u) buf[((size_t)r * ns + j++) * n + i] = st1[u];
+        if (slots & 4u) buf[((size_t)r * ns + j++) * n + i] = st2[u];
+        if (slots & 8u) buf[((size_t)r * ns + j++) * n + i] = st3[u];
+    }
+}
 
 // propagate flags
 #define PF_ZERO_SLOT 1u  // zero the ring count of slot t (classic order: update(t) fills it next)
@@ -1092,6 +1120,16 @@ cudaError_t update_smem(const NetDev& d, int bs, K kernel, size_t* bytes)
     return cudaSuccess;
 }
 
+// the state monitor's record of step clock + k_off (when a monitor is set)
+cudaError_t launch_monitor(szsnn_net* n, const NetDev& d, int k_off, cudaStream_t st)
+{
+    if (!n->mon_n) return cudaSuccess;
+    const int grid = (int)std::min<int64_t>(sz_div_up(n->mon_n, 256), 1024);
+    k_monitor<<<grid, 256, 0, st>>>(d.clock, k_off, n->d_mon_t0, d.st0, d.st1, d.st2, d.st3, n->d_mon_ids, n->mon_n,
+                                    n->mon_slots, n->d_mon_buf, (long long)n->mon_cap);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_update(szsnn_net* n, const NetDev& d, int k_off, const uint32_t* forced, const float* cur,
                           uint32_t* words, cudaStream_t st)
 {
@@ -1159,6 +1197,9 @@ void free_net(szsnn_net* n)
     cudaFree(n->d_blk_pop);
     cudaFree(n->d_row_ptr);
     cudaFree(n->d_rp_dm);
+    cudaFree(n->d_mon_ids);
+    cudaFree(n->d_mon_buf);
+    cudaFree(n->d_mon_t0);
     cudaFree(n->d_syn);
     for (int k = 0; k < 4; ++k) cudaFree(n->d_st[k]);
     for (int p = 0; p < 2; ++p) {
@@ -1473,9 +1514,10 @@ extern "C" int szsnn_net_step(szsnn_net* n, const uint32_t* forced_host, const f
         NET_TRY(n, launch_propagate_classic(n, d, 0, st));
         NET_TRY(n, launch_update(n, d, 0, forced, cur, n->d_raster_stage[0], st));
     }
+    NET_TRY(n, launch_monitor(n, d, 0, st));
     k_advance<<<1, 1, 0, st>>>(n->d_clock, 1);
     NET_TRY(n, cudaGetLastError());
-    n->kernel_launches += n->overlap ? 2 : 3;
+    n->kernel_launches += (n->overlap ? 2 : 3) + (n->mon_n ? 1 : 0);
     n->steps_done += 1;
     if (fired_host) {
         NET_TRY(n, cudaMemcpyAsync(n->h_pinned_words, n->d_raster_stage[0], (size_t)n->words * 4, cudaMemcpyDeviceToHost, st));
@@ -1509,6 +1551,7 @@ static int net_graph(szsnn_net* n, int len, int flags, int b, cudaGraphExec_t* o
             e = launch_propagate_classic(n, d, k, st);
             if (e == cudaSuccess) e = launch_update(n, d, k, fw, cu, ras, st);
         }
+        if (e == cudaSuccess) e = launch_monitor(n, d, k, st);
     }
     if (e == cudaSuccess) {
         k_advance<<<1, 1, 0, st>>>(n->d_clock, len);
@@ -1645,7 +1688,7 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
         NET_TRY(n, cudaGraphLaunch(ex, st));
         NET_TRY(n, cudaEventRecord(n->ev_comp[b], st));
         n->graph_launches += 1;
-        n->kernel_launches += (uint64_t)(n->overlap ? 1 : 2) * len + 1;
+        n->kernel_launches += (uint64_t)((n->overlap ? 1 : 2) + (n->mon_n ? 1 : 0)) * len + 1;
         if (raster) {
             rc = flush(b);  // bounce b last held chunk k-2
             if (rc) return rc;
@@ -1877,6 +1920,61 @@ extern "C" int szsnn_net_get_state(szsnn_net* n, int slot, float* host)
     return SZSNN_OK;
 }
 
+extern "C" int szsnn_net_set_monitor(szsnn_net* n, const int32_t* ids, int32_t n_ids, uint32_t slot_mask,
+                                     int64_t capacity)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    if (n_ids < 0 || (n_ids > 0 && (!ids || slot_mask == 0 || slot_mask > 15u || capacity < 1)))
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG,
+                               "szsnn_net_set_monitor: ids, a slot mask in 1..15 and a capacity >= 1 are needed");
+    for (int32_t i = 0; i < n_ids; ++i)
+        if (ids[i] < 0 || ids[i] >= n->U)
+            return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "szsnn_net_set_monitor: unit id outside 0..U-1");
+    cudaStream_t st = n->ctx->stream;
+    NET_TRY(n, cudaStreamSynchronize(st));  // no step in flight writes the old trace
+    cudaFree(n->d_mon_ids);
+    cudaFree(n->d_mon_buf);
+    n->d_mon_ids = nullptr;
+    n->d_mon_buf = nullptr;
+    n->mon_n = 0;
+    n->mon_slots = 0;
+    n->mon_cap = 0;
+    for (auto& kv : n->graphs) cudaGraphExecDestroy(kv.second);  // graphs hold the monitor launches or not
+    n->graphs.clear();
+    if (n_ids == 0) return SZSNN_OK;
+    const size_t ns = (size_t)__builtin_popcount(slot_mask);
+    NET_TRY(n, dalloc(&n->d_mon_ids, (size_t)n_ids));
+    NET_TRY(n, dalloc(&n->d_mon_buf, (size_t)capacity * ns * (size_t)n_ids));
+    if (!n->d_mon_t0) NET_TRY(n, dalloc(&n->d_mon_t0, 1));
+    n->mon_t0 = n->steps_done;
+    NET_TRY(n, cudaMemcpyAsync(n->d_mon_ids, ids, (size_t)n_ids * 4, cudaMemcpyHostToDevice, st));
+    NET_TRY(n, cudaMemcpyAsync(n->d_mon_t0, &n->mon_t0, 8, cudaMemcpyHostToDevice, st));
+    NET_TRY(n, cudaStreamSynchronize(st));
+    n->mon_n = n_ids;
+    n->mon_slots = slot_mask;
+    n->mon_cap = capacity;
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_monitor_read(szsnn_net* n, float* out, int64_t max_steps, int64_t* steps_out,
+                                      int64_t* dropped_out)
+{
+    if (!n || max_steps < 0 || (max_steps > 0 && !out)) return SZSNN_ERR_ARG;
+    if (!n->mon_n) return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "szsnn_net_monitor_read: no monitor is set");
+    cudaStream_t st = n->ctx->stream;
+    const int64_t recorded = n->steps_done - n->mon_t0;
+    const int64_t kept = std::min<int64_t>(recorded, n->mon_cap);
+    const int64_t steps = std::min<int64_t>(kept, max_steps);
+    const size_t row = (size_t)__builtin_popcount(n->mon_slots) * (size_t)n->mon_n;
+    if (steps > 0) NET_TRY(n, cudaMemcpyAsync(out, n->d_mon_buf, (size_t)steps * row * 4, cudaMemcpyDeviceToHost, st));
+    n->mon_t0 = n->steps_done;  // recording restarts at the current step
+    NET_TRY(n, cudaMemcpyAsync(n->d_mon_t0, &n->mon_t0, 8, cudaMemcpyHostToDevice, st));
+    NET_TRY(n, cudaStreamSynchronize(st));
+    if (steps_out) *steps_out = steps;
+    if (dropped_out) *dropped_out = recorded - steps;
+    return SZSNN_OK;
+}
+
 extern "C" int szsnn_net_set_state(szsnn_net* n, int slot, const float* host)
 {
     if (!n || slot < 0 || slot > 3 || !host) return SZSNN_ERR_ARG;
@@ -1943,6 +2041,11 @@ extern "C" int szsnn_net_restore(szsnn_net* n, const void* blob, uint64_t bytes)
     NET_TRY(n, cudaMemcpyAsync(n->d_clock, &clock, 8, cudaMemcpyHostToDevice, st));
     NET_TRY(n, cudaStreamSynchronize(st));
     n->steps_done = clock;
+    if (n->mon_n) {  // the monitor's trace restarts at the restored step
+        n->mon_t0 = clock;
+        NET_TRY(n, cudaMemcpyAsync(n->d_mon_t0, &n->mon_t0, 8, cudaMemcpyHostToDevice, st));
+        NET_TRY(n, cudaStreamSynchronize(st));
+    }
     return net_prime(n);
 }
 

@@ -173,6 +173,32 @@ class Network:
         L.check(self.lib.szsnn_net_run_device(self.h, steps, forced_ptr, current_ptr, raster_ptr), self.ctx.h,
                 "net_run_device")
 
+    def set_monitor(self, ids, slots=(0,), capacity: int = 1000) -> None:
+        """Record state slots `slots` of units `ids` after every step, on the
+        device, for up to `capacity` steps between reads (ids=[] turns it off)."""
+        ids = np.ascontiguousarray(ids, np.int32)
+        mask = 0
+        for k in slots:
+            if not 0 <= int(k) <= 3:
+                raise ValueError("state slots are 0..3")
+            mask |= 1 << int(k)
+        self._mon = (len(ids), bin(mask).count("1"), int(capacity)) if len(ids) else None
+        L.check(self.lib.szsnn_net_set_monitor(self.h, ids.ctypes.data if len(ids) else None, len(ids), mask,
+                                               int(capacity)), self.ctx.h, "set_monitor")
+
+    def monitor_read(self) -> tuple[np.ndarray, int]:
+        """(trace [steps, slots, units] fp32 since set_monitor or the last read,
+        steps not recorded because they ran past the capacity); recording then
+        restarts at the current step."""
+        if getattr(self, "_mon", None) is None:
+            raise ValueError("no monitor is set")
+        n, ns, cap = self._mon
+        out = np.zeros((cap, ns, n), np.float32)
+        steps, dropped = C.c_int64(), C.c_int64()
+        L.check(self.lib.szsnn_net_monitor_read(self.h, out.ctypes.data, cap, C.byref(steps), C.byref(dropped)),
+                self.ctx.h, "monitor_read")
+        return out[: steps.value].copy(), int(dropped.value)
+
     def device_ms(self) -> float:
         """Device time (CUDA events on the net's stream) of the last run / run_device."""
         t = C.c_double()
