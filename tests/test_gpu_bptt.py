@@ -154,3 +154,26 @@ def test_checkpoint_interval_does_not_change_gradients():
         ymax.sum().backward()
         grads.append(w_in.grad.clone())
     assert torch.equal(grads[0], grads[1])
+
+
+def test_full_size_gradients_do_not_depend_on_the_checkpoint_interval():
+    """The benchmark's BPTT shape (10,000 neurons, 10 % recurrent, 700 inputs,
+    20 readouts, batch 64) over 100 steps: recomputing from checkpoints every
+    25 or every 50 steps gives bit-identical input and recurrent weight
+    gradients (a size-independent check of the recompute and of the recurrent
+    term).  The readout-weight gradient is summed with fp32 atomics (its order
+    varies from run to run), so it is compared within 1e-6 relative."""
+    grads = []
+    for ck in (25, 50):
+        net, w_in, val, w_out, x, v0 = _setup(N=10000, M=700, K=20, B=64, T=100, ck=ck, seed=11)
+        for t in (w_in, val, w_out):
+            t.requires_grad_(True)
+        ymax, vsum = P.LIFCurrExpFunction.apply(w_in, val, w_out, x, v0, net)
+        (ymax.sum() + 1e-3 * vsum.sum()).backward()
+        torch.cuda.synchronize()
+        grads.append([t.grad.clone() for t in (w_in, val, w_out)])
+    for g0, g1 in zip(*grads):
+        assert torch.isfinite(g0).all() and float(g0.abs().max()) > 0
+    assert torch.equal(grads[0][0], grads[1][0]) and torch.equal(grads[0][1], grads[1][1])
+    g0, g1 = grads[0][2], grads[1][2]
+    assert float((g0 - g1).abs().max()) <= 1e-6 * float(g0.abs().max())
