@@ -344,8 +344,8 @@ int szsnn_net_timing(szsnn_net* net, double* propagate_ms, double* update_ms, do
  * (threads, a multiple of 32 in 32..256; each thread updates 4 units) */
 int szsnn_net_set_tuning(szsnn_net* net, int propagate_mode, int group, int propagate_blocks, int update_block);
 /* Step order.  1 (default): overlapped -- input buffers double-buffered by
- * step parity, delivery of delays >= 2 into step t+1 runs on a second stream
- * while update(t) runs, and update(t) delivers the delay-1 bucket of its own
+ * step parity, delivery of delays >= 2 into step t+1 runs in the same launch
+ * as update(t), and update(t) delivers the delay-1 bucket of its own
  * spikes.  0: classic -- propagate(t) delivers delays 1..D, then update(t)
  * (the reference's order, Simulation.ipp:471-496).  Results are identical in
  * fixed-point accumulation; switching mid-run rebuilds the next step's
