@@ -275,16 +275,38 @@ def bench_bptt(args):
 
 
 def run_reference(args, rank):
+    """The reference arm: the oracle port of the reference's step (all host
+    threads) on the bounded CPU sample of the benchmark network.  One bench
+    step is S simulation steps of the sample, S = ceil(2000 / K), so the K
+    timed steps cover at least 2000 simulation steps and at most K; the W
+    warm-up steps (W * S simulation steps, at least 100) fill the delay ring."""
     if rank != 0:
         return
-    cb = cpu_baseline(args)
-    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.cpu_steps, "warmup": 100, "higher_is_better": True, "scaling": "weak",
+    import oracle
+    import szsnn_b200 as sz  # noqa: F401
+
+    K, W = max(1, args.steps), max(1, args.warmup)
+    S = max(1, -(-2000 // K))
+    threads = os.cpu_count() or 1
+    n, p, D, blocks, pops = cond_config(args.cpu_neurons, args.fanout)
+    csr = oracle.generate(blocks, args.seed, n + p, D)
+    on = oracle.OracleNet(n, p, D, pops, csr, state=init_state(n, p, args.seed))
+    on.run(max(W * S, 100), nthreads=threads)
+    t0 = time.perf_counter()
+    _, ev = on.run(K * S, nthreads=threads)
+    dt = time.perf_counter() - t0
+    value = ev / dt
+    cb = {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+          "sample": f"{n} IF_cond_exp neurons x {args.fanout} synapses + {p} Poisson x 100, same weights, "
+                    f"delays and rates as the 1M network; {K} steps of {S} simulation steps after "
+                    f"{max(W * S, 100)} warm-up simulation steps; {ev} events in {dt:.2f} s"}
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": K, "warmup": W, "ms_per_step": dt / K * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "IF_cond_exp 1M x 1000 syn, Poisson 100k x 100, dt 0.1 ms (bounded CPU sample)",
-                       "neurons": args.cpu_neurons},
+                       "neurons": args.cpu_neurons, "sim_steps_per_step": S},
             "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
