@@ -445,6 +445,10 @@ __device__ __forceinline__ void update_spikes(const NetDev& nd, long long t, int
     const int64_t wd = id >> 5;
     if (lane == 0 && out_words && wd < nd.words) out_words[wd] = ball;
     if (ball) {
+        // the delay-1 bucket bounds are loaded before the ring append, so the
+        // two round trips overlap
+        unsigned long long ra = 0, re = 0;
+        if (nd.overlap && spk) bucket_bounds(nd, nd.rp_dm && __popc(ball) >= 8, id, 1, ra, re);
         const int R = nd.D + 1;
         const int64_t slot = t % R;
         uint32_t base = 0;
@@ -463,10 +467,6 @@ __device__ __forceinline__ void update_spikes(const NetDev& nd, long long t, int
             // trips rather than one per unit
             constexpr int NEAR_UNR = 2;
             const InBuf nb = in_buf(nd, t + 1);
-            unsigned long long ra = 0, re = 0;
-            if (spk) {
-                bucket_bounds(nd, nd.rp_dm && __popc(ball) >= 8, id, 1, ra, re);
-            }
             const uint32_t len = (uint32_t)(re - ra);
             uint32_t incl = len;
 #pragma unroll
