@@ -51,7 +51,7 @@ NCU_STEP_TRAFFIC_FANOUT100 = 70_663_936
 NCU_STEP_EVENTS_FANOUT100 = 245_471
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10000)
@@ -79,7 +79,7 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=1000)
     ap.add_argument("--bptt-scale", type=float, default=1.0)
     ap.add_argument("--bptt-steps", type=int, default=500)
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def cond_config(n: int, fanout: int):

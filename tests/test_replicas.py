@@ -64,3 +64,19 @@ def test_reference_arm_other_ranks_do_nothing(capsys):
     import bench
     bench.run_reference(None, rank=1)
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_reports_the_steps_it_was_given(capsys):
+    """The reference arm's line carries the K timed and W warm-up steps of its
+    command line, each step S = ceil(2000 / K) simulation steps of the CPU
+    sample, and its value is the sample's events over the timed steps."""
+    import json
+    sys.path.insert(0, ROOT)
+    import bench
+    args = bench.parse(["--impl", "reference", "--steps", "3", "--warmup", "4", "--cpu-neurons", "2000"])
+    bench.run_reference(args, rank=0)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["steps"] == 3 and line["warmup"] == 4
+    assert line["config"]["sim_steps_per_step"] == 667
+    assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
