@@ -597,12 +597,9 @@ __device__ __forceinline__ bool tile_load(const NetDev& nd, const InBuf& inb, in
                                           const TileSmem& sm)
 {
     if (MODEL == SZSNN_POISSON) return true;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0) {  // init, then the copies at once; the block barrier below orders the waits after the init
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(sm.bar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
         const int64_t n = min((int64_t)T, nd.U - tile0);  // the tile lies inside a neuron population
         const uint32_t b4 = (uint32_t)((n * 4 + 15) & ~(int64_t)15);
         const uint32_t b8 = (uint32_t)((n * 8 + 15) & ~(int64_t)15);
@@ -620,6 +617,7 @@ __device__ __forceinline__ bool tile_load(const NetDev& nd, const InBuf& inb, in
             bulk_load(sm.ii, inb.i + tile0, b4, sm.bar);
         }
     }
+    __syncthreads();
     if (tile_wait(sm.bar)) return true;
     // the copies did not complete in time: report, wait once more so none is
     // still writing shared memory when the block leaves, skip the tile
