@@ -43,11 +43,11 @@ BYTES_PER_NEURON = 48    # 16 B state read + 16 B write + 8 B input read + 8 B c
 # DRAM bytes (read + write) per launch from single ncu captures (cold L2):
 # k_update at 1.1M units, the benchmark's unit count; k_propagate at 300k
 # neurons x 1000 synapses (152,640 events per launch), scaled by events.
-NCU_UPDATE_TRAFFIC = 25_418_752
+NCU_UPDATE_TRAFFIC = 25_399_040
 NCU_PROPAGATE_TRAFFIC_PER_EVENT = 5_706_752 / 152_640
 # k_step at 1.1M units and fan-out 100 (245,471 events per launch): 70.7 MB; the per-(spike, delay)
 # item traffic is the same at fan-out 1000, each further event adds its 8 B synapse
-NCU_STEP_TRAFFIC_FANOUT100 = 70_663_936
+NCU_STEP_TRAFFIC_FANOUT100 = 70_680_320
 NCU_STEP_EVENTS_FANOUT100 = 245_471
 
 
