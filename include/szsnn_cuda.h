@@ -412,7 +412,12 @@ int szsnn_bptt_backward(const szsnn_bptt_desc* d, char* err, size_t err_len);
  * The first call on a device looks up the array's device address (make it
  * before any stream capture).  Every call shares the array and clears what
  * must start at zero; calls that overlap on the GPU race on it and must be
- * serialised by the caller.  The call is asynchronous on `stream`. */
+ * serialised by the caller.  The call is asynchronous on `stream`; the
+ * population table and the step number travel as kernel parameters, so
+ * nothing is read from this struct after the call returns.  Device-side
+ * errors (a synapse target outside the neurons, a full ring slot) are
+ * recorded in `error_word`, which is required: zero it before the first
+ * call; the first error stays there until the caller clears it. */
 #define SZSNN_STATIC_MAX_NEURONS 262144
 typedef struct {
     int64_t  n_neurons, n_sources;
@@ -429,7 +434,7 @@ typedef struct {
     uint32_t* ring_cnt;         /* device, D+1, zero before the first step */
     int32_t*  ring_ids;         /* device, (D+1)*(N+P) */
     uint32_t* fired_words;      /* device out, (N+P+31)/32 spike words, or NULL */
-    uint32_t* error_word;       /* device out, 2 words (code, info), or NULL */
+    uint32_t* error_word;       /* device in/out, 2 words (code, info); required, sticky */
     void*     stream;           /* cudaStream_t, NULL = legacy default stream */
 } szsnn_static_step;
 int szsnn_step_static(const szsnn_static_step* s, char* err, size_t err_len);

@@ -26,12 +26,17 @@ def build_oracle(force: bool = False) -> str:
     return lib
 
 
-def build_all(force: bool = False) -> None:
+def build_all(ref_root: str | None = None, force: bool = False) -> None:
+    """The C restatement always; the reference's kernels under the emulator
+    when a reference checkout is given (argument or SZSNN_REFERENCE)."""
     build_oracle(force)
-    from .clemu.build_clemu import REF_ROOT, build_clemu
-    if os.path.isdir(REF_ROOT):
-        build_clemu(force)
+    from .clemu.build_clemu import build_clemu, cl_dir, reference_root
+    ref_root = ref_root or reference_root()
+    if ref_root and os.path.isdir(cl_dir(ref_root)):
+        build_clemu(ref_root, force)
 
 
 if __name__ == "__main__":
-    build_all(force="--force" in sys.argv)
+    # usage: python -m oracle.build [<reference root>] [--force]
+    args = [a for a in sys.argv[1:] if a != "--force"]
+    build_all(args[0] if args else None, force="--force" in sys.argv)

@@ -43,8 +43,17 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE = os.path.dirname(HERE)
 OUT = os.path.join(ORACLE, "_ref")
-REF_ROOT = os.environ.get("SZSNN_REFERENCE", "/root/reference")
-CL_DIR = os.path.join(REF_ROOT, "szsnn1.1", "src", "cl")
+
+
+def reference_root() -> str | None:
+    """The reference checkout to read the kernel sources from: the
+    SZSNN_REFERENCE environment variable, or None (the prebuilt libraries in
+    oracle/_ref/ are then used as they are)."""
+    return os.environ.get("SZSNN_REFERENCE") or None
+
+
+def cl_dir(ref_root: str) -> str:
+    return os.path.join(ref_root, "szsnn1.1", "src", "cl")
 
 VARIANTS = {
     # name: (MAX_PARTITION_SIZE, WARP_SIZE, NEURONS_PER_WI, MAX_SYNAPTIC_DELAY)
@@ -161,11 +170,21 @@ def _stale(target, deps):
     return not os.path.exists(target) or any(os.path.getmtime(d) > os.path.getmtime(target) for d in deps)
 
 
-def build_variant(name: str, force: bool = False) -> str:
+def build_variant(name: str, force: bool = False, ref_root: str | None = None) -> str:
+    """Build oracle/_ref/libclemu_<name>.so from the kernel sources under
+    `ref_root` (default: reference_root()).  Without a reference checkout an
+    existing library is returned as it is; a missing one is an error."""
     mps, warp, npw, delay = VARIANTS[name]
+    lib = os.path.join(OUT, f"libclemu_{name}.so")
+    ref_root = ref_root or reference_root()
+    if ref_root is None:
+        if os.path.exists(lib):
+            return lib
+        raise FileNotFoundError(f"{lib} is not built and no reference checkout is given "
+                                "(set SZSNN_REFERENCE to the reference's root directory)")
+    CL_DIR = cl_dir(ref_root)
     gen = os.path.join(OUT, "gen", name)
     os.makedirs(gen, exist_ok=True)
-    lib = os.path.join(OUT, f"libclemu_{name}.so")
     deps = [os.path.join(HERE, "clemu_rt.cpp"), os.path.join(HERE, "clemu_rt.hpp"), os.path.abspath(__file__)]
     deps += [os.path.join(CL_DIR, f) for f, _, _ in KERNELS.values()]
     if not force and not _stale(lib, deps):
@@ -193,12 +212,17 @@ def build_variant(name: str, force: bool = False) -> str:
     return lib
 
 
-def build_clemu(force: bool = False) -> list[str]:
-    if not os.path.isdir(CL_DIR):
-        raise FileNotFoundError(f"reference kernel sources not found under {CL_DIR}")
-    return [build_variant(v, force) for v in VARIANTS]
+def build_clemu(ref_root: str, force: bool = False) -> list[str]:
+    if not os.path.isdir(cl_dir(ref_root)):
+        raise FileNotFoundError(f"reference kernel sources not found under {cl_dir(ref_root)}")
+    return [build_variant(v, force, ref_root) for v in VARIANTS]
 
 
 if __name__ == "__main__":
-    for p in build_clemu(force="--force" in sys.argv):
+    # usage: python -m oracle.clemu.build_clemu <reference root> [--force]
+    args = [a for a in sys.argv[1:] if a != "--force"]
+    root = args[0] if args else reference_root()
+    if not root:
+        sys.exit("usage: build_clemu.py <reference root> [--force]  (or set SZSNN_REFERENCE)")
+    for p in build_clemu(root, force="--force" in sys.argv):
         print(p)

@@ -24,7 +24,6 @@ SOURCES = [
     "context.cu",
     "ref_kernels.cu",
     "net.cu",
-    "batch.cu",
     "bptt.cu",
     "layout.cpp",
 ]
@@ -59,7 +58,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(ROOT, "include", "szsnn_cuda.h"))
     objs = []
-    srcs = [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    missing = [s for s in SOURCES if not os.path.exists(os.path.join(CSRC, s))]
+    if missing:
+        raise FileNotFoundError(f"listed sources missing from {CSRC}: {', '.join(missing)}")
+    srcs = list(SOURCES)
     for s in srcs:
         src = os.path.join(CSRC, s)
         obj = os.path.join(objdir, s + ".o")

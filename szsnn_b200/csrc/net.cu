@@ -2134,6 +2134,21 @@ extern "C" int szsnn_net_last_inputs(szsnn_net* n, float* in_exc, float* in_inh)
 static __device__ __align__(256) unsigned char
     g_static_scratch[SZSNN_STATIC_HDR_BYTES + 2 * sizeof(float) * SZSNN_STATIC_MAX_NEURONS];
 
+// Header of one call, written by a kernel whose parameters carry the
+// population table and the step number by value (nothing is read from host
+// memory after the call returns): [0] step counter, [64] statistics zeroed,
+// [256] population table.
+__global__ void k_static_setup(PopDev p0, PopDev p1, long long clock, unsigned char* base)
+{
+    const int w = (int)(sizeof(PopDev) / 8);
+    unsigned long long* tab = reinterpret_cast<unsigned long long*>(base + 256);
+    const unsigned long long* a = reinterpret_cast<const unsigned long long*>(&p0);
+    const unsigned long long* b = reinterpret_cast<const unsigned long long*>(&p1);
+    for (int i = threadIdx.x; i < 2 * w; i += blockDim.x) tab[i] = i < w ? a[i] : b[i - w];
+    if (threadIdx.x < 8) reinterpret_cast<unsigned long long*>(base + 64)[threadIdx.x] = 0ull;
+    if (threadIdx.x == 0) *reinterpret_cast<long long*>(base) = clock;
+}
+
 #include <mutex>
 
 namespace {
@@ -2169,6 +2184,9 @@ extern "C" int szsnn_step_static(const szsnn_static_step* s, char* err, size_t e
     if (!s->row_ptr || (!s->syn && U > 0) || !s->state[0] || !s->state[1] || !s->state[2] || !s->state[3] ||
         !s->ring_cnt || !s->ring_ids)
         return static_fail(err, err_len, SZSNN_ERR_ARG, "szsnn_step_static: null device buffer");
+    if (!s->error_word)
+        return static_fail(err, err_len, SZSNN_ERR_ARG,
+                           "szsnn_step_static: error_word is required (device errors are reported there)");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= 64)
@@ -2194,21 +2212,19 @@ extern "C" int szsnn_step_static(const szsnn_static_step* s, char* err, size_t e
         sms = g_static_sms[dev];
     }
     cudaStream_t st = (cudaStream_t)s->stream;
-    // header layout: [0] step counter, [64] statistics, [128] error word, [256] population table
+    // header layout: [0] step counter, [64] statistics, [256] population table
     PopDev hp[2];
     std::memset(hp, 0, sizeof(hp));
     hp[0].model = s->model; hp[0].flags = s->flags; hp[0].begin = 0; hp[0].end = N;
     std::memcpy(hp[0].p, s->params, sizeof(s->params));
     if (s->model != SZSNN_IZHIKEVICH) { hp[0].p[12] = sz_decay(s->params[4]); hp[0].p[13] = sz_decay(s->params[5]); }
     hp[1].model = SZSNN_POISSON; hp[1].begin = N; hp[1].end = U; hp[1].p[0] = s->source_p; hp[1].seed = s->seed;
-    const long long clock = s->step;
     float* acc = (float*)(base + SZSNN_STATIC_HDR_BYTES);
-    e = cudaMemcpyAsync(base + 256, hp, sizeof(hp), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(base, &clock, sizeof(clock), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(base + 64, 0, 64 + 8, st);       // statistics and error word
+    k_static_setup<<<1, 64, 0, st>>>(hp[0], hp[1], (long long)s->step, base);
+    e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, 2 * sizeof(float) * (size_t)N, st);  // input accumulators
     if (e != cudaSuccess)
-        return static_fail(err, err_len, SZSNN_ERR_CUDA, std::string("szsnn_step_static: set-up copy: ") + cudaGetErrorString(e));
+        return static_fail(err, err_len, SZSNN_ERR_CUDA, std::string("szsnn_step_static: set-up: ") + cudaGetErrorString(e));
     NetDev d{};
     d.N = N; d.U = U; d.words = sz_div_up(U, 32); d.D = D; d.npops = P > 0 ? 2 : 1;
     d.pops = (const PopDev*)(base + 256);
@@ -2220,7 +2236,7 @@ extern "C" int szsnn_step_static(const szsnn_static_step* s, char* err, size_t e
     d.ring_cnt = s->ring_cnt; d.ring_ids = s->ring_ids;
     d.clock = (const long long*)base;
     d.stats = (unsigned long long*)(base + 64);
-    d.err = s->error_word ? s->error_word : (uint32_t*)(base + 128);
+    d.err = s->error_word;
     d.upt = 1;
     k_propagate<16><<<sms * 16, 256, 0, st>>>(d, 0, 1, PF_ZERO_SLOT | PF_SPIKES);
     e = cudaGetLastError();

@@ -1,7 +1,7 @@
 """Extract golden vectors from the reference's known-answer files.
 
 Run once where the reference tree is present:
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py <reference root>
 It writes small .npz fixtures beside this script; the tests only read those.
 
 Sources (paths inside the reference project):
@@ -82,4 +82,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference root>")
+    main(sys.argv[1])
