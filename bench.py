@@ -1,19 +1,24 @@
 #!/usr/bin/env python
 """Benchmark: synaptic events/s of the 1M-neuron IF_cond_exp network on B200.
 
-Workload (the large IF_cond_exp configuration): 1,000,000 IF_cond_exp neurons
-(800k excitatory / 200k inhibitory), 1000 random synapses per neuron (1e9
-synapses; targets uniform without self-loops; weights exc ~U(0,4) nS, inh
-~U(0,51) nS stored negative; delays U{1..64} steps), e_rev_E 0, e_rev_I -80 mV,
-tau_syn_E 5, tau_syn_I 10 ms, dt 0.1 ms, 100,000 Poisson inputs at 5 Hz with
-100 targets each, fp32 state.  Parameters the configuration leaves open are
-taken from the 4000-neuron IF_curr_exp configuration (tau_m 20 ms, cm 0.2 nF,
-v_rest -60, v_thresh -50, v_reset -60 mV, tau_refrac 5 ms); Poisson synapses
-~U(0,100) nS with delay 1 step; v(0) ~ U(-60,-50) mV.  Conductances in uS.
+Workload (the large IF_cond_exp configuration, szsnn_b200.workloads.cond_config):
+1,000,000 IF_cond_exp neurons (800k excitatory / 200k inhibitory), 1000 random
+synapses per neuron (1e9 synapses; targets uniform without self-loops; weights
+exc ~U(0,4) nS, inh ~U(0,51) nS stored negative; delays U{1..64} steps),
+e_rev_E 0, e_rev_I -80 mV, tau_syn_E 5, tau_syn_I 10 ms, dt 0.1 ms, 100,000
+Poisson inputs at 5 Hz with 100 targets each, fp32 state.  Parameters the
+configuration leaves open are taken from the 4000-neuron IF_curr_exp
+configuration (tau_m 20 ms, cm 0.2 nF, v_rest -60, v_thresh -50, v_reset
+-60 mV, tau_refrac 5 ms); Poisson synapses ~U(0,100) nS with delay 1 step;
+v(0) ~ U(-60,-50) mV.  Conductances in uS.
 
-A step = one simulation time step (propagate + update); the network is built
-on the device by the fixed fan-out generator.  Inputs are larger than L2
-(8 GB synapse table); the per-neuron state (16 MB) stays L2-resident across
+Timing.  `--steps K` timed steps, `--warmup W` warm-up steps; one step is S
+simulation time steps (propagate + update), S = ceil(20,000 / K) on the GPU
+(ceil(2000 / K) in the CPU reference arm), so every timed region covers at
+least 20,000 (2000) simulation steps.  `ms_per_step` is per SIMULATION step;
+the timed region is steps x sim_steps_per_step of them.  The network is built
+on the device by the fixed fan-out generator; inputs are larger than L2 (8 GB
+synapse table), and the per-neuron state (16 MB) stays L2-resident across
 steps as it does in any run of this network.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -38,6 +43,10 @@ import numpy as np  # noqa: E402
 METRIC = "syn-events/s @1M IF_cond_exp"
 UNIT = "syn-events/s"
 DT_MS = 0.1
+GPU_SIM_STEPS = 20_000   # least simulation steps in the GPU arm's timed region
+REF_SIM_STEPS = 2_000    # least simulation steps in the CPU reference arm's timed region
+CPU_WARM_STEPS = 500     # oracle warm-up simulation steps (past the v(0) volley and its echo)
+CPU_TIMED_STEPS = 200    # simulation steps timed by the cpu_baseline leg
 BYTES_PER_EVENT = 8      # int32 target + fp32 weight, delay implied by the bucket
 BYTES_PER_NEURON = 48    # 16 B state read + 16 B write + 8 B input read + 8 B clear
 # DRAM bytes (read + write) per launch from single ncu captures (cold L2):
@@ -54,13 +63,16 @@ NCU_STEP_EVENTS_FANOUT100 = 245_471
 def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10000)
-    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--neurons", type=int, default=1_000_000)
     ap.add_argument("--fanout", type=int, default=1000)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--acc", default="float", choices=["float", "fixed"])
+    ap.add_argument("--sim-steps", type=int, default=None,
+                    help="least simulation steps in the timed region (default 20000 on the GPU, 2000 in the "
+                         "reference arm); one timed step is ceil(this / --steps) simulation steps")
     ap.add_argument("--classic", dest="overlap", action="store_false",
                     help="propagate-then-update order (two launches per step) instead of the overlapped one")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
@@ -69,11 +81,12 @@ def parse(argv=None):
     ap.add_argument("--shape", default=None,
                     help="fixed launch shape 'order,mode,group,blocks,update_block' (order: overlapped|classic) "
                          "instead of the tuner")
-    ap.add_argument("--e2e-steps", type=int, default=1000)
+    ap.add_argument("--e2e-steps", type=int, default=2000)
     ap.add_argument("--profile-steps", type=int, default=200)
-    ap.add_argument("--cpu-neurons", type=int, default=50_000)
-    ap.add_argument("--cpu-steps", type=int, default=300)
+    ap.add_argument("--cpu-neurons", type=int, default=None,
+                    help="neurons of the network the CPU port runs (default: the benchmark's own --neurons)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the 1000-neuron and 4000-neuron configurations")
     ap.add_argument("--no-secondary", action="store_true", help="skip the batched-sweep and BPTT measurements")
     ap.add_argument("--batch-nets", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=1000)
@@ -82,54 +95,88 @@ def parse(argv=None):
     return ap.parse_args(argv)
 
 
-def cond_config(n: int, fanout: int):
-    """Generator blocks, populations and initial state of the benchmark network."""
-    import szsnn_b200 as sz
-    from szsnn_b200.network import GenBlock
+def sim_steps_per_step(k: int, least: int) -> int:
+    """S: simulation steps in one timed step so that k of them cover `least`."""
+    return max(1, -(-least // max(1, k)))
 
-    p = n // 10
-    D = 64
-    ne = int(0.8 * n)
-    blocks = [GenBlock(0, ne, 0, n, fanout, 0.0, 0.004, 1.0, 1, D, True, 1),
-              GenBlock(ne, n - ne, 0, n, fanout, 0.0, 0.051, -1.0, 1, D, True, 2),
-              GenBlock(n, p, 0, n, 100, 0.0, 0.1, 1.0, 1, 1, False, 3)]
-    pv = sz.fold_dt(sz.if_params(v_rest=-60, cm=0.2, tau_m=20, tau_refrac=5, tau_syn_E=5, tau_syn_I=10,
-                                 v_reset=-60, v_thresh=-50, e_rev_E=0.0, e_rev_I=-80.0), DT_MS)
-    pops = [sz.Pop(sz.IF_COND_EXP, 0, n, pv),
-            sz.Pop(sz.POISSON, n, n + p, np.array([5.0 * DT_MS * 1e-3], np.float32), seed=20240)]
-    return n, p, D, blocks, pops
+
+def cond_config(n: int, fanout: int):
+    from szsnn_b200.workloads import cond_config as cc
+    return cc(n, fanout)
 
 
 def init_state(n, p, seed):
-    rng = np.random.default_rng(seed)
-    v0 = np.concatenate([rng.uniform(-60, -50, n), np.zeros(p)]).astype(np.float32)
-    fired = np.concatenate([np.full(n, 1e4), np.zeros(p)]).astype(np.float32)
-    return [v0, None, None, fired]
+    from szsnn_b200.workloads import init_state as ist
+    return ist(n, p, seed)
+
+
+def headline_config(n, p, D, n_syn, acc):
+    """The workload description both arms report (identical keys and values
+    when both run the same network)."""
+    return {"workload": "IF_cond_exp 1M neurons x 1000 synapses (1e9), 100k Poisson x 100, "
+                        "delays U{1..64} steps, dt 0.1 ms",
+            "neurons": n, "sources": p, "synapses": int(n_syn), "max_delay": D, "accumulation": acc,
+            "l2": "inputs larger than L2 (8 GB synapse table); neuron state L2-resident across steps"}
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks, power and throttle reasons sampled during the timed region
+    (NVML, read-only, every 20 ms; nvidia-smi every 100 ms when NVML is not
+    importable).  The device is found by the CUDA device's UUID."""
 
-    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    HW, HW_THERMAL, SW_THERMAL, SW_POWER = 0x8, 0x40, 0x20, 0x4
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
+        self.samples = []  # (sm_mhz, max_mhz, reasons bitmask)
         self._stop = threading.Event()
         self._t = None
+        self._nv = None
+        self._h = None
+        try:
+            import pynvml as nv
+            import torch
+            nv.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(index).uuid)
+            for cand in (uuid, "GPU-" + uuid):
+                try:
+                    self._h = nv.nvmlDeviceGetHandleByUUID(cand)
+                    break
+                except Exception:
+                    continue
+            if self._h is None:
+                self._h = nv.nvmlDeviceGetHandleByIndex(index)
+            self._nv = nv
+        except Exception:
+            self._nv = None
+
+    def _sample_nvml(self):
+        nv, h = self._nv, self._h
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        return float(sm), float(mx), int(rs)
+
+    def _sample_smi(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits"],
+                             capture_output=True, text=True, timeout=5)
+        f = [x.strip() for x in out.stdout.strip().splitlines()[0].split(",")]
+        bits = 0
+        for flag, v in zip((self.HW, self.HW_THERMAL, self.SW_THERMAL, self.SW_POWER), f[2:6]):
+            if v.lower() in ("active", "1"):
+                bits |= flag
+        return float(f[0]), float(f[1]), bits
 
     def _run(self):
+        period = 0.02 if self._nv else 0.1
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                line = out.stdout.strip().splitlines()[0]
-                self.samples.append([x.strip() for x in line.split(",")])
+                self.samples.append(self._sample_nvml() if self._nv else self._sample_smi())
             except Exception:
                 pass
-            self._stop.wait(0.1)
+            self._stop.wait(period)
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -143,13 +190,12 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and
-                          s[3 + i].lower() in ("active", "1")})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        sm = [s[0] for s in self.samples]
+        names = {self.HW: "hw_slowdown", self.HW_THERMAL: "hw_thermal_slowdown",
+                 self.SW_THERMAL: "sw_thermal_slowdown", self.SW_POWER: "sw_power_cap"}
+        reasons = sorted({nm for s in self.samples for bit, nm in names.items() if s[2] & bit})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": reasons, "samples": len(self.samples), "source": "nvml" if self._nv else "nvidia-smi"}
 
 
 def peaks():
@@ -161,35 +207,169 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def net_overlap(net) -> bool:
-    """The step order the network runs in (set by --classic or by the tuner)."""
-    return bool(net.overlap)
-
-
 def pinned_words(steps, words):
     """uint32 [steps, words] in page-locked host memory (torch's pinned allocator)."""
     import torch
     return torch.empty((steps, words), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
 
 
-def cpu_baseline(args, n_steps_warm=100):
-    """Oracle port, all host threads, on a bounded sample of the same network."""
+def cpu_port_measure(n, fanout, seed, warm, timed, threads=None):
+    """The oracle port of the reference's step on the benchmark network of n
+    neurons (all host threads): generated with the GPU generator's algorithm
+    and seed, `warm` untimed simulation steps, then `timed` timed ones.
+    Returns (events/s, events, seconds, description)."""
     import oracle
-    import szsnn_b200 as sz  # noqa: F401
 
-    threads = os.cpu_count() or 1
-    n, p, D, blocks, pops = cond_config(args.cpu_neurons, args.fanout)
-    csr = oracle.generate(blocks, args.seed, n + p, D)
-    on = oracle.OracleNet(n, p, D, pops, csr, state=init_state(n, p, args.seed))
-    on.run(n_steps_warm, nthreads=threads)
+    threads = threads or os.cpu_count() or 1
+    n, p, D, blocks, pops = cond_config(n, fanout)
     t0 = time.perf_counter()
-    steps = max(args.cpu_steps - n_steps_warm, 50)
-    _, ev = on.run(steps, nthreads=threads)
+    csr = oracle.generate(blocks, seed, n + p, D)
+    gen_s = time.perf_counter() - t0
+    on = oracle.OracleNet(n, p, D, pops, csr, state=init_state(n, p, seed))
+    on.run(warm, nthreads=threads)
+    t0 = time.perf_counter()
+    _, ev = on.run(timed, nthreads=threads)
     dt = time.perf_counter() - t0
-    return {"value": ev / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} IF_cond_exp neurons x {args.fanout} synapses + {p} Poisson x 100, same weights, "
-                      f"delays and rates as the 1M network; {steps} steps after {n_steps_warm} warm-up steps; "
-                      f"{ev} events in {dt:.2f} s"}
+    desc = (f"{n} IF_cond_exp neurons x {fanout} synapses + {p} Poisson x 100 (the benchmark network, same "
+            f"generator and seed); {timed} simulation steps timed after {warm} warm-up steps; {ev} events in "
+            f"{dt:.2f} s on {threads} threads (generation {gen_s:.1f} s, untimed)")
+    del on, csr
+    return ev / dt, ev, dt, desc, threads
+
+
+def cpu_baseline(args):
+    """The oracle port on the benchmark network itself: 500 warm-up and 200
+    timed simulation steps (the reference arm's procedure, shorter)."""
+    n = args.cpu_neurons or args.neurons
+    v, ev, dt, desc, threads = cpu_port_measure(n, args.fanout, args.seed, CPU_WARM_STEPS, CPU_TIMED_STEPS)
+    return {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc,
+            "same_network": n == args.neurons}
+
+
+def bench_configs(ctx, args):
+    """The 1000-neuron Izhikevich and 4000-neuron IF_curr_exp configurations:
+    syn-events/s, neuron-updates/s and device time per 1000 simulation steps
+    (the reference's published unit) on the GPU, with CPU baselines in the
+    same run: the reference's own kernels under the work-group emulator
+    (Oracle B, one host thread: the emulator runs work-groups in turn) on a
+    bounded sample, and the oracle port on all host threads."""
+    import oracle
+    import szsnn_b200 as sz
+    from szsnn_b200 import workloads as WL
+
+    hbm, _ = peaks()
+    out = {}
+
+    def gpu_run(net, steps, n_units, bytes_per_unit, current_ptr=None):
+        net.run_device(steps, current_ptr=current_ptr)  # warm-up: graphs, transient
+        ctx.sync()
+        s0 = net.stats()
+        net.run_device(steps, current_ptr=current_ptr)
+        ctx.sync()
+        ms = net.device_ms()
+        s1 = net.stats()
+        ev = s1["events"] - s0["events"]
+        us = ms / steps * 1e3
+        return {"syn_events_per_s": ev / (ms * 1e-3), "neuron_updates_per_s": n_units * steps / (ms * 1e-3),
+                "ms_per_1000_steps": ms / steps * 1000.0, "us_per_step": us, "steps": steps,
+                "events_per_step": ev / steps,
+                "roofline_hbm_frac": (n_units * bytes_per_unit + ev / steps * BYTES_PER_EVENT) / (us * 1e-6) / 1e9
+                / hbm,
+                "bound": "launch and latency: one fused kernel per step over a few thousand units"}
+
+    # configuration 1: Izhikevich 1000, 2 x 0.5 ms half-steps, thalamic input
+    izh = WL.izh_network(n=1000, seed=5)
+    n = izh["n"]
+    pops, csr, st = WL.izh_native(izh)
+    pops[0].flags = sz.POP_IZH_HALF_STEPS
+    steps1 = 1000
+    cur = WL.thalamic(n, izh["ne"], steps1, seed=9)
+    net = sz.Network(ctx, n, 0, izh["D"], pops, csr=csr, state=st, graph_chunk=100)
+    dcur = ctx.upload(cur)
+    g1 = gpu_run(net, steps1, n, 16, current_ptr=dcur.ptr)  # v, u read + write
+    net.close()
+    dcur.free()
+    c1 = {"gpu": g1}
+    # oracle port, all threads, full 1000 steps
+    on = oracle.OracleNet(n, 0, izh["D"], pops, csr, state=st)
+    t0 = time.perf_counter()
+    _, ev = on.run(steps1, current=cur, nthreads=os.cpu_count())
+    dt = time.perf_counter() - t0
+    c1["cpu_port"] = {"ms_per_1000_steps": dt / steps1 * 1e6, "syn_events_per_s": ev / dt,
+                      "neuron_updates_per_s": n * steps1 / dt, "cores": os.cpu_count(), "kind": "port",
+                      "sample": f"all {steps1} steps, 2 x 0.5 ms half-steps"}
+    # the reference's own kernels (single 1 ms step, the reference's rule), bounded sample
+    try:
+        import oracle.clemu as clemu
+        from szsnn_b200 import _lib as L
+        consts = L.LayoutConsts(1024, 256, 32, 64)
+        params = np.stack([izh["a"], izh["b"], izh["c"], izh["d"]], 1)
+        vars_ = np.stack([izh["v0"], izh["u0"]], 1)
+        sim = sz.RefSimulation(clemu.ClemuBackend("prod"), consts, "Izhikevich", params, vars_, izh["src"],
+                               izh["tgt"], izh["w"], izh["d1"])
+        kb = 60
+        spikes = 0
+        t0 = time.perf_counter()
+        for k in range(kb):
+            spikes += len(sim.step_and_fired(None, cur[k]))
+        dt = time.perf_counter() - t0
+        evb = spikes * 100  # every spike of this network reaches its 100 targets
+        c1["cpu_reference_kernels"] = {
+            "ms_per_1000_steps": dt / kb * 1e6, "syn_events_per_s": evb / dt,
+            "neuron_updates_per_s": n * kb / dt, "cores": 1, "kind": "reference",
+            "sample": f"first {kb} of {steps1} steps (single 1 ms steps, the reference's Izhikevich rule), "
+                      "reference kernels under the work-group emulator, driven by the Simulation mirror"}
+    except Exception as e:  # the emulator library is built only where the reference tree was present
+        c1["cpu_reference_kernels"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    out["izh1000"] = c1
+
+    # configuration 2: IF_curr_exp 4000, delays U{1..100}, 1000 Poisson at 10 Hz, 10,000 steps
+    w = WL.if4000(seed=11)
+    steps2 = 10_000
+    net = sz.Network(ctx, w["n"], w["p"], w["D"], w["pops"], csr=w["csr"], state=w["state"], graph_chunk=100)
+    g2 = gpu_run(net, steps2, w["n"] + w["p"], 48)
+    net.close()
+    c2 = {"gpu": g2}
+    on = oracle.OracleNet(w["n"], w["p"], w["D"], w["pops"], w["csr"], state=w["state"])
+    t0 = time.perf_counter()
+    _, ev = on.run(steps2, nthreads=os.cpu_count())
+    dt = time.perf_counter() - t0
+    c2["cpu_port"] = {"ms_per_1000_steps": dt / steps2 * 1e6, "syn_events_per_s": ev / dt,
+                      "neuron_updates_per_s": (w["n"] + w["p"]) * steps2 / dt, "cores": os.cpu_count(),
+                      "kind": "port", "sample": f"all {steps2} steps"}
+    # the reference's kernels on the variant its layout holds (delays <= 64): the
+    # Poisson trains drawn on the host, forced onto an input partition
+    try:
+        import oracle.clemu as clemu
+        from szsnn_b200 import _lib as L
+        wb = WL.if4000(seed=11, clip_delay=63)  # stored delays 2..64
+        nn, pp = wb["n"], wb["p"]
+        consts = L.LayoutConsts(1024, 256, 32, 64)
+        params = np.tile(WL.if4000_params()[:9], (nn, 1))
+        vars_ = np.stack([wb["state"][0][:nn], np.zeros(nn), np.zeros(nn), np.full(nn, 1e4)], 1).astype(np.float32)
+        in_base = -(-nn // 1024) * 1024
+        src = np.where(wb["src"] >= nn, wb["src"] - nn + in_base, wb["src"])
+        sim = sz.RefSimulation(clemu.ClemuBackend("prod"), consts, "IF_curr_exp", params, vars_, src, wb["tgt"],
+                               wb["w"], wb["d1"], input_params=np.zeros((pp, 1), np.float32),
+                               input_vars=np.zeros((pp, 1), np.float32))
+        rng = np.random.default_rng(3)
+        kb = 300
+        spikes = 0
+        t0 = time.perf_counter()
+        for k in range(kb):
+            ids = in_base + np.nonzero(rng.random(pp) < wb["p_step"])[0]
+            spikes += len(sim.step_and_fired(ids if len(ids) else None))
+        dt = time.perf_counter() - t0
+        c2["cpu_reference_kernels"] = {
+            "ms_per_1000_steps": dt / kb * 1e6, "neuron_updates_per_s": (nn + pp) * kb / dt,
+            "cores": 1, "kind": "reference",
+            "sample": f"first {kb} of {steps2} steps of the delays <= 64 variant (the reference layout's "
+                      "limit), Poisson trains forced onto an input partition, reference kernels under the "
+                      "work-group emulator"}
+    except Exception as e:
+        c2["cpu_reference_kernels"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    out["if4000"] = c2
+    return out
 
 
 def bench_batched(ctx, args):
@@ -203,15 +383,17 @@ def bench_batched(ctx, args):
     specs = B.sweep_specs(args.batch_nets, seed=0)
     r = B.compare_batched_looped(ctx, specs, steps=args.batch_steps, graph_chunk=100, tune=True)
     same = bool(np.array_equal(r["spikes_batched"], r["spikes_looped"]))
-    return {"metric": "nets/s (batched sweep)", "nets": r["nets"], "steps": r["steps"],
-            "batched_nets_per_s": r["batched_nets_per_s"], "looped_nets_per_s": r["looped_nets_per_s"],
-            "speedup": r["speedup"], "batched_s": r["batched_s"], "looped_s": r["looped_s"],
-            "wall_batched_s": r["wall_batched_s"], "wall_looped_s": r["wall_looped_s"],
-            "neurons": r["neurons"], "synapses": r["synapses"],
-            "syn_events_per_s_batched": r["events_batched"] / r["batched_s"],
-            "spike_counts_equal_looped": same, "accumulation": "float",
-            "workload": f"{r['nets']} nets, N log-uniform 200..20000, fan-out 100, delays U{{1..20}} steps, "
-                        f"w scale 0.5..2.0, Poisson 5..20 Hz, dt 1 ms, {r['steps']} steps"}
+    keys = ("nets", "steps", "batched_nets_per_s", "looped_nets_per_s", "speedup", "batched_s", "looped_s",
+            "wall_batched_s", "wall_looped_s", "neurons", "synapses")
+    res = {"metric": "nets/s (batched sweep)", **{k: r[k] for k in keys},
+           "syn_events_per_s_batched": r["events_batched"] / r["batched_s"],
+           "spike_counts_equal_looped": same, "accumulation": "float",
+           "workload": f"{r['nets']} nets, N log-uniform 200..20000, fan-out 100, delays U{{1..20}} steps, "
+                       f"w scale 0.5..2.0, Poisson 5..20 Hz, dt 1 ms, {r['steps']} steps"}
+    for k in ("looped_tuned_s", "looped_tuned_nets_per_s", "speedup_vs_tuned_loop", "loop_tuning"):
+        if k in r:
+            res[k] = r[k]
+    return res
 
 
 def bench_bptt(args):
@@ -276,35 +458,23 @@ def bench_bptt(args):
 
 def run_reference(args, rank):
     """The reference arm: the oracle port of the reference's step (all host
-    threads) on the bounded CPU sample of the benchmark network.  One bench
-    step is S simulation steps of the sample, S = ceil(2000 / K), so the K
-    timed steps cover at least 2000 simulation steps and at most K; the W
-    warm-up steps (W * S simulation steps, at least 100) fill the delay ring."""
+    threads) on the benchmark network itself (--cpu-neurons overrides its
+    size).  One step is S simulation steps, S = ceil(2000 / K), so the K
+    timed steps cover at least 2000 simulation steps; the warm-up is
+    max(500, W * S) simulation steps, past the start-up volley."""
     if rank != 0:
         return
-    import oracle
-    import szsnn_b200 as sz  # noqa: F401
-
     K, W = max(1, args.steps), max(1, args.warmup)
-    S = max(1, -(-2000 // K))
-    threads = os.cpu_count() or 1
-    n, p, D, blocks, pops = cond_config(args.cpu_neurons, args.fanout)
-    csr = oracle.generate(blocks, args.seed, n + p, D)
-    on = oracle.OracleNet(n, p, D, pops, csr, state=init_state(n, p, args.seed))
-    on.run(max(W * S, 100), nthreads=threads)
-    t0 = time.perf_counter()
-    _, ev = on.run(K * S, nthreads=threads)
-    dt = time.perf_counter() - t0
-    value = ev / dt
-    cb = {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-          "sample": f"{n} IF_cond_exp neurons x {args.fanout} synapses + {p} Poisson x 100, same weights, "
-                    f"delays and rates as the 1M network; {K} steps of {S} simulation steps after "
-                    f"{max(W * S, 100)} warm-up simulation steps; {ev} events in {dt:.2f} s"}
+    S = sim_steps_per_step(K, args.sim_steps or REF_SIM_STEPS)
+    n = args.cpu_neurons or args.neurons
+    warm = max(CPU_WARM_STEPS, W * S)
+    value, ev, dt, desc, threads = cpu_port_measure(n, args.fanout, args.seed, warm, K * S)
+    nn, p, D, _, _ = cond_config(n, args.fanout)
+    cb = {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": K, "warmup": W, "ms_per_step": dt / K * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "IF_cond_exp 1M x 1000 syn, Poisson 100k x 100, dt 0.1 ms (bounded CPU sample)",
-                       "neurons": args.cpu_neurons, "sim_steps_per_step": S},
+            "steps": K, "warmup": W, "ms_per_step": dt / (K * S) * 1e3, "sim_steps_per_step": S,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": headline_config(nn, p, D, nn * args.fanout + p * 100, "float"),
             "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -351,7 +521,8 @@ def main():
         if dist is not None:
             dist.barrier()
 
-
+    K, W = max(1, args.steps), max(1, args.warmup)
+    S = sim_steps_per_step(K, args.sim_steps or GPU_SIM_STEPS)
     ctx = sz.Context(local_rank)
     n, p, D, blocks, pops = cond_config(args.neurons, args.fanout)
     acc = L.ACC_FIXED if args.acc == "fixed" else L.ACC_FLOAT
@@ -361,9 +532,10 @@ def main():
     net.set_overlap(args.overlap)
     gen_s = time.perf_counter() - t0
 
-    # warm-up (graph instantiation, initial transient), then the launch shape
-    # chosen by the autotuner on replays of a warmed-up step (scratch state)
-    net.run_device(args.warmup)
+    # warm-up: W x S simulation steps (graph capture, the start-up transient),
+    # then the launch shape chosen by the autotuner on replays of a warmed-up
+    # step (scratch state), then W x S more steps in the chosen shape
+    net.run_device(W * S)
     ctx.sync()
     tuning = None
     if args.shape:
@@ -372,47 +544,43 @@ def main():
         net.set_tuning(int(mode), int(group), int(blocks_), int(ub))
         tuning = {"overlap": order == "overlapped", "mode": int(mode), "group": int(group), "blocks": int(blocks_),
                   "update_block": int(ub), "source": "--shape"}
-        net.run_device(args.warmup)
-        ctx.sync()
     elif args.tune:  # past the start-up transient (v(0) ~ U(-60,-50) fires a first volley)
         from szsnn_b200.autotune import tune
-        net.run_device(max(0, args.tune_after - args.warmup))
+        net.run_device(max(0, args.tune_after - W * S))
         ctx.sync()
         ch = tune(net, replays=50, use_cache=False)
         tuning = {k: ch[k] for k in ("overlap", "mode", "group", "blocks", "update_block", "step_us",
                                      "classic_step_us")}
-        net.run_device(args.warmup)  # graphs of the chosen shape
-        ctx.sync()
-    overlap = net_overlap(net)
+    net.run_device(W * S)
+    ctx.sync()
+    overlap = bool(net.overlap)
     s0 = net.stats()
     barrier()
     ctx.sync()
-    import ctypes as C
-    lib = L.lib()
-    # CUDA events on the net's stream, through torch if present, else via the library timing
+    # timed: K x S simulation steps in CUDA graphs (every graph already
+    # instantiated: szsnn_net_run_device builds them before its first event);
+    # CUDA events on the net's stream around the launches
     with ClockSampler(local_rank) as clk:
         t_wall = time.perf_counter()
-        net.run_device(args.steps)
+        net.run_device(K * S)
         ctx.sync()
         t_wall = time.perf_counter() - t_wall
-        _, _, total_ms = (C.c_double(), C.c_double(), C.c_double())
-        pm, um, tm = C.c_double(), C.c_double(), C.c_double()
-        lib.szsnn_net_timing(net.h, C.byref(pm), C.byref(um), C.byref(tm))
+    ms_timed = net.device_ms()
     barrier()
     s1 = net.stats()
-    ms_timed = tm.value if tm.value > 0 else t_wall * 1e3
+    sim_steps = K * S
     events = s1["events"] - s0["events"]
     spikes = s1["spikes"] - s0["spikes"]
     ms_max, ev_tot = reduce_replicas(dist, ms_timed, events)
     value = ev_tot / (ms_max / 1e3)
+    us_live = ms_max / sim_steps * 1e3
 
     # end to end through the public API: host input words in, host raster out,
     # every step, both in page-locked host memory (DMA overlapped with compute)
-    e2e_steps = min(args.e2e_steps, args.steps)
+    e2e_steps = min(args.e2e_steps, sim_steps)
     forced, raster = pinned_words(e2e_steps, net.words), pinned_words(e2e_steps, net.words)
     forced[:] = 0
-    # untimed warm-up through the same call: the graphs of host-I/O chunks (both
-    # stage buffers) are captured and instantiated once, outside the timed run
+    # untimed warm-up through the same call (its graphs and bounce paths)
     warm = min(e2e_steps, 2 * net.graph_chunk)
     net.run(warm, forced_words=forced[:warm], out=raster[:warm])
     ctx.sync()
@@ -436,51 +604,53 @@ def main():
     prop_us = prof["propagate_ms"] / steps_p * 1e3
     upd_us = prof["update_ms"] / steps_p * 1e3
     step_us = prof["step_ms"] / steps_p * 1e3
-    prop_bytes = ev_launch * BYTES_PER_EVENT
+    ev_step = events / sim_steps
     upd_bytes = n * BYTES_PER_NEURON
-    ev_step = events / args.steps
-    if overlap:
-        # one fused launch per step (k_step): the update of every unit, the
-        # delay-1 buckets of its spikes and the delay >= 2 delivery of the next step
-        step_bytes = upd_bytes + ev_step * BYTES_PER_EVENT
-        dom = {"kernel": "k_step", "achieved": step_bytes / (step_us * 1e-6) / 1e9, "bytes_per_launch": step_bytes,
-               "us_per_launch": step_us,
-               "traffic": int(NCU_STEP_TRAFFIC_FANOUT100 + max(0.0, ev_step - NCU_STEP_EVENTS_FANOUT100) * 8)
-               if n + p == 1_100_000 else None}
-    elif prop_us >= upd_us:
-        dom = {"kernel": "k_propagate", "achieved": prop_bytes / (prop_us * 1e-6) / 1e9,
-               "bytes_per_launch": prop_bytes, "us_per_launch": prop_us,
-               "traffic": int(NCU_PROPAGATE_TRAFFIC_PER_EVENT * ev_launch)}
-    else:
-        dom = {"kernel": "k_update", "achieved": upd_bytes / (upd_us * 1e-6) / 1e9, "bytes_per_launch": upd_bytes,
-               "us_per_launch": upd_us, "traffic": NCU_UPDATE_TRAFFIC if n + p == 1_100_000 else None}
-    roofline = {"bound": "hbm", "achieved": round(dom["achieved"], 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(dom["achieved"] / hbm, 4), "traffic": dom["traffic"], "kernel": dom["kernel"],
-                "peak_source": peak_kind,
-                "us_per_launch": round(dom["us_per_launch"], 3),
-                "algorithmic_bytes_per_launch": int(dom["bytes_per_launch"]),
-                "step": {"us": round(step_us, 3), "order": "overlapped" if overlap else "classic"},
-                "delivery_alone": {"us_per_launch": round(prop_us, 3),
-                                   "gbs": round(prop_bytes / (prop_us * 1e-6) / 1e9, 1),
-                                   "events_per_launch": ev_launch,
-                                   "delays": "2..64" if overlap else "1..64"},
-                "update_alone": {"us_per_launch": round(upd_us, 3),
-                                 "gbs": round(upd_bytes / (upd_us * 1e-6) / 1e9, 1)}}
+    step_bytes = upd_bytes + ev_step * BYTES_PER_EVENT
+    chip = ctx.probe_peaks(n)  # measured L2 copy bandwidth and random-reduction rate
+    # the dominant kernel: k_step (one fused launch per step: the update of
+    # every unit, the delay-1 buckets of its spikes and the delay >= 2
+    # delivery of the next step) in the overlapped order; its live time per
+    # launch is the timed region's time per simulation step
+    traffic = (int(NCU_STEP_TRAFFIC_FANOUT100 + max(0.0, ev_step - NCU_STEP_EVENTS_FANOUT100) * 8)
+               if (n + p == 1_100_000 and overlap) else None)
+    achieved = step_bytes / (us_live * 1e-6) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "traffic": traffic,
+                "kernel": "k_step" if overlap else "k_propagate + k_update", "peak_source": peak_kind,
+                "us_per_launch": round(us_live, 3), "algorithmic_bytes_per_launch": int(step_bytes),
+                "timing": "live: the timed region's device time per simulation step",
+                "l2_gbs_peak": round(chip["l2_copy_gbs"], 1),
+                "l2_frac": round(achieved / chip["l2_copy_gbs"], 4),
+                "atomic_per_s_peak": chip["red_per_s"],
+                "atomic_frac": round(ev_step / (us_live * 1e-6) / chip["red_per_s"], 4),
+                "ceilings": "l2_gbs_peak: L2-resident copy of 2 x 16 MB; atomic_per_s_peak: random fp32 red into "
+                            "2 x N floats (szsnn_probe_peaks, this device, this run)",
+                "replays": {"step_us": round(step_us, 3), "order": "overlapped" if overlap else "classic",
+                            "delivery_alone_us": round(prop_us, 3), "delivery_events": ev_launch,
+                            "delivery_gbs": round(ev_launch * BYTES_PER_EVENT / (prop_us * 1e-6) / 1e9, 1),
+                            "delays": "2..64" if overlap else "1..64",
+                            "update_alone_us": round(upd_us, 3),
+                            "update_gbs": round(upd_bytes / (upd_us * 1e-6) / 1e9, 1)}}
+    n_syn, words = net.n_synapses, net.words
+    net.close()  # frees the 8 GB synapse table before the other workloads
 
+    configs = batched = bptt = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        try:
+            configs = bench_configs(ctx, args)
+        except Exception as e:  # reported beside the headline, not required for it
+            configs = {"error": f"{type(e).__name__}: {e}"}
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             cb = cpu_baseline(args)
         except Exception as e:  # the baseline is reported, not required
             cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
-
-    n_syn, words = net.n_synapses, net.words
-    net.close()  # frees the 8 GB synapse table before the secondary workloads
-    batched = bptt = None
     if rank == 0 and world == 1 and not args.no_secondary:
         try:
             batched = bench_batched(ctx, args)
-        except Exception as e:  # reported beside the headline, not required for it
+        except Exception as e:
             batched = {"error": f"{type(e).__name__}: {e}"}
         try:
             bptt = bench_bptt(args)
@@ -488,29 +658,26 @@ def main():
             bptt = {"error": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
-        steps = args.steps
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "IF_cond_exp 1M neurons x 1000 synapses (1e9), 100k Poisson x 100, "
-                                   "delays U{1..64} steps, dt 0.1 ms",
-                       "neurons": n, "sources": p, "synapses": n_syn, "max_delay": D,
-                       "accumulation": args.acc, "graph_chunk": 100,
-                       "step_order": "overlapped" if overlap else "classic", "tuning": tuning,
-                       "l2": "inputs larger than L2 (8 GB synapse table); neuron state L2-resident across steps",
-                       "parallelism": f"replicas x{world}"},
-            "neuron_updates_per_s": (n + p) * steps * world / (ms_max / 1e3),
-            "mean_rate_hz": spikes / max(n + p, 1) / (steps * DT_MS * 1e-3),
-            "events_per_step": events / steps,
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms_max / sim_steps, "sim_steps_per_step": S, "sim_steps_timed": sim_steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": headline_config(n, p, D, n_syn, args.acc),
+            "parallelism": f"replicas x{world}", "step_order": "overlapped" if overlap else "classic",
+            "graph_chunk": 100, "tuning": tuning,
+            "neuron_updates_per_s": (n + p) * sim_steps * world / (ms_max / 1e3),
+            "mean_rate_hz": spikes / max(n + p, 1) / (sim_steps * DT_MS * 1e-3),
+            "events_per_step": events / sim_steps,
+            "wall_s_timed": t_wall,
             "generate_s": gen_s,
             "roofline": roofline,
             "cpu_baseline": cb,
             "e2e": {"value": e2e_tot / e2e_max, "unit": UNIT, "steps": e2e_steps,
                     "h2d_bytes_per_step": int(words * 4), "d2h_bytes_per_step": int(words * 4),
                     "api": "szsnn_net_run (forced-spike words in, raster out, page-locked host arrays)"},
-            "gpu_launches": int((1 if overlap else 2) * steps + (steps + 99) // 100),
+            "gpu_launches": int((1 if overlap else 2) * sim_steps + (sim_steps + 99) // 100),
             "clocks": clk.summary(),
+            "configs": configs,
             "batched": batched,
             "bptt": bptt,
         }

@@ -397,6 +397,22 @@ int szsnn_bptt_workspace_bytes(const szsnn_bptt_desc* d, uint64_t* bytes);
 int szsnn_bptt_forward(const szsnn_bptt_desc* d, char* err, size_t err_len);
 int szsnn_bptt_backward(const szsnn_bptt_desc* d, char* err, size_t err_len);
 
+/* ------------------------------------------------------ measured ceilings ---
+ * No counterpart in the reference.  The step keeps its neuron state and input
+ * accumulators in L2 across steps and does one fp32 reduction per synaptic
+ * event at a random target, so its roofline denominators are on-chip rates,
+ * measured here on the device of `ctx`: an L2-resident copy (two 16 MB
+ * buffers, read + write bytes per second) and random `red.add.f32` into
+ * 2 * n_targets floats (reductions per second).  Synchronous; allocates and
+ * frees its own buffers. */
+typedef struct {
+    double  l2_copy_gbs;     /* read + write GB/s of the L2-resident copy        */
+    int64_t l2_copy_bytes;   /* bytes of the two copy buffers                   */
+    double  red_per_s;       /* random fp32 reductions per second               */
+    int64_t red_targets;     /* floats the reductions land in                   */
+} szsnn_peaks;
+int szsnn_probe_peaks(szsnn_ctx* ctx, int64_t n_targets, szsnn_peaks* out);
+
 /* ----------------------------------------- allocation-free single step ---
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory -- hosts that own and partition all of it (a fixed-budget pool or

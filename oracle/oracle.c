@@ -60,12 +60,17 @@ static inline int orc_poisson_fires(uint64_t seed, int64_t idx, int64_t step, fl
 }
 
 /* ---- fixed fan-out generator ------------------------------------------- */
+/* Rows are independent (row r owns synapses base + [0, F)), so they are
+ * generated in parallel; each thread keeps its own delay histogram. */
 void orc_gen_fixed_fanout(const orc_gen_block* b, uint64_t seed, int32_t D,
                           uint64_t* row_ptr, int32_t* tgt, float* w)
 {
     const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
     const int F = b->fanout;
+#pragma omp parallel
+    {
     uint32_t* cnt = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(D + 1));
+#pragma omp for schedule(static, 1024)
     for (int64_t r = 0; r < b->src_count; ++r) {
         const int64_t s = b->src_begin + r;
         const uint64_t base = b->syn_offset + (uint64_t)r * (uint64_t)F;
@@ -103,6 +108,7 @@ void orc_gen_fixed_fanout(const orc_gen_block* b, uint64_t seed, int32_t D,
         }
     }
     free(cnt);
+    }
 }
 
 /* ---- the step, instantiated for fp32 and fp64 --------------------------- */

@@ -80,6 +80,11 @@ class NetStats(C.Structure):
                 ("graph_launches", C.c_uint64), ("kernel_launches", C.c_uint64)]
 
 
+class Peaks(C.Structure):
+    _fields_ = [("l2_copy_gbs", C.c_double), ("l2_copy_bytes", C.c_int64), ("red_per_s", C.c_double),
+                ("red_targets", C.c_int64)]
+
+
 _lib = None
 
 # name -> (restype, argtypes); every entry point declared in include/szsnn_cuda.h
@@ -133,6 +138,7 @@ SIGNATURES = {
     "szsnn_net_set_tuning": (_I, [_P, _I, _I, _I, _I]),
     "szsnn_net_set_overlap": (_I, [_P, C.c_int]),
     "szsnn_step_static": (_I, [_P, C.c_char_p, C.c_size_t]),
+    "szsnn_probe_peaks": (_I, [_P, _I64, _P]),
     "szsnn_bptt_workspace_bytes": (_I, [_P, C.POINTER(C.c_uint64)]),
     "szsnn_bptt_forward": (_I, [_P, C.c_char_p, C.c_size_t]),
     "szsnn_bptt_backward": (_I, [_P, C.c_char_p, C.c_size_t]),

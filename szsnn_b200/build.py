@@ -25,6 +25,7 @@ SOURCES = [
     "ref_kernels.cu",
     "net.cu",
     "bptt.cu",
+    "probe.cu",
     "layout.cpp",
 ]
 

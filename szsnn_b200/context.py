@@ -72,6 +72,15 @@ class Context:
     def sync(self) -> None:
         L.check(L.lib().szsnn_sync(self.h), self.h, "sync")
 
+    def probe_peaks(self, n_targets: int = 1_000_000) -> dict:
+        """Measured on-chip ceilings of this device (szsnn_probe_peaks): the
+        L2-resident copy bandwidth and the random fp32 reduction rate into
+        2 * n_targets floats."""
+        p = L.Peaks()
+        L.check(L.lib().szsnn_probe_peaks(self.h, int(n_targets), C.byref(p)), self.h, "probe_peaks")
+        return {"l2_copy_gbs": p.l2_copy_gbs, "l2_copy_bytes": p.l2_copy_bytes, "red_per_s": p.red_per_s,
+                "red_targets": p.red_targets}
+
     def device_error(self) -> tuple[int, int]:
         code, info = C.c_uint32(), C.c_uint32()
         L.check(L.lib().szsnn_device_error(self.h, C.byref(code), C.byref(info)), self.h, "device_error")

@@ -1012,7 +1012,8 @@ int upd_upt(const szsnn_net* n)
     return (int)std::max<int64_t>(1, std::min<int64_t>(UPD_UPT, per_sm / 4));
 }
 
-NetDev make_dev(szsnn_net* n)
+// par: parity of the step counter when the launches built from this run
+NetDev make_dev(szsnn_net* n, int par)
 {
     NetDev d{};
     d.N = n->N; d.U = n->U; d.words = n->words; d.D = n->D; d.npops = n->npops;
@@ -1026,7 +1027,7 @@ NetDev make_dev(szsnn_net* n)
     d.dbg_in_e = nullptr; d.dbg_in_i = nullptr;
     d.group = n->d_group; d.group_spikes = n->d_group_spikes;
     d.blk_pop = n->d_blk_pop;
-    d.par0 = (uint32_t)(n->steps_done & 1);
+    d.par0 = (uint32_t)(par & 1);
     d.upt = upd_upt(n);
     // parameter-table slots: the populations with shared parameters and a model
     // the inline update covers, each with the update blocks that lie inside it
@@ -1046,6 +1047,8 @@ NetDev make_dev(szsnn_net* n)
     }
     return d;
 }
+
+NetDev make_dev(szsnn_net* n) { return make_dev(n, (int)(n->steps_done & 1)); }
 
 // delivery of delays m_lo..D into the inputs of step clock + k_off
 cudaError_t launch_propagate(szsnn_net* n, const NetDev& d, int k_off, int m_lo, uint32_t pf, cudaStream_t st)
@@ -1525,17 +1528,18 @@ extern "C" int szsnn_net_step(szsnn_net* n, const uint32_t* forced_host, const f
     return SZSNN_OK;
 }
 
-// graph of `len` steps; flags bit0 forced, bit1 current, bit2 raster; `b`
-// selects the forced / raster stage buffers.  Overlapped order: one k_step
-// per step (on entry the inputs of the first step are complete: its far
-// delivery ran in the previous step's launch, or at priming).
-static int net_graph(szsnn_net* n, int len, int flags, int b, cudaGraphExec_t* out)
+// graph of `len` steps starting at a step of parity `par`; flags bit0
+// forced, bit1 current, bit2 raster; `b` selects the forced / raster stage
+// buffers.  Overlapped order: one k_step per step (on entry the inputs of the
+// first step are complete: its far delivery ran in the previous step's
+// launch, or at priming).
+static int net_graph(szsnn_net* n, int len, int flags, int b, int par, cudaGraphExec_t* out)
 {
-    auto key = std::make_tuple(len, flags, b, (int)(n->steps_done & 1));
+    auto key = std::make_tuple(len, flags, b, par & 1);
     auto it = n->graphs.find(key);
     if (it != n->graphs.end()) { *out = it->second; return SZSNN_OK; }
     cudaStream_t st = n->ctx->stream;
-    NetDev d = make_dev(n);
+    NetDev d = make_dev(n, par);
     cudaGraph_t g = nullptr;
     NET_TRY(n, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
@@ -1635,6 +1639,29 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
         const bool need = q < 2 ? bounce_in : bounce_out;
         if (need && !n->h_io[q]) NET_TRY(n, cudaMallocHost((void**)&n->h_io[q], (size_t)n->chunk * wbytes));
     }
+    // Host runs with copies: a short first chunk (its input copy cannot overlap
+    // compute) and a short last chunk (nor can its raster copy), chunk / 8
+    // steps each, so the pipeline fills and drains quickly.
+    const bool edges = host && (forced || raster) && steps >= 2 * (int64_t)n->chunk;
+    const int64_t edge = std::max<int64_t>(1, n->chunk / 8);
+    const int flags = (forced ? 1 : 0) | (current ? 2 : 0) | (raster ? 4 : 0);
+    // the chunk plan, and every graph it needs captured and instantiated
+    // before the run's first event: graph building never falls inside the
+    // device time the run reports
+    std::vector<std::pair<int, cudaGraphExec_t>> plan;
+    for (int64_t done = 0, k = 0; done < steps; ++k) {
+        const int64_t left = steps - done;
+        int len = (int)std::min<int64_t>(n->chunk, left);
+        if (edges) {
+            if (k == 0 || left <= edge) len = (int)std::min<int64_t>(edge, left);
+            else if (left < n->chunk + edge) len = (int)(left - edge);
+        }
+        cudaGraphExec_t ex = nullptr;
+        int rc = net_graph(n, len, flags, (int)(k & 1), (int)((n->steps_done + done) & 1), &ex);
+        if (rc) return rc;
+        plan.emplace_back(len, ex);
+        done += len;
+    }
     NET_TRY(n, cudaEventRecord(n->ev_run0, st));
     NET_TRY(n, cudaStreamWaitEvent(cp, n->ev_run0, 0));  // copies follow earlier work on the main stream
     NET_TRY(n, cudaStreamWaitEvent(cpo, n->ev_run0, 0));
@@ -1649,21 +1676,10 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
         pend[b].on = false;
         return SZSNN_OK;
     };
-    // Host runs with copies: a short first chunk (its input copy cannot overlap
-    // compute) and a short last chunk (nor can its raster copy), chunk / 8
-    // steps each, so the pipeline fills and drains quickly.
-    const bool edges = host && (forced || raster) && steps >= 2 * (int64_t)n->chunk;
-    const int64_t edge = std::max<int64_t>(1, n->chunk / 8);
-    int64_t k = 0;
-    for (int64_t done = 0; done < steps; ++k) {
+    int64_t done = 0;
+    for (size_t k = 0; k < plan.size(); ++k) {
         const int b = (int)(k & 1);
-        const int64_t left = steps - done;
-        int len = (int)std::min<int64_t>(n->chunk, left);
-        if (edges) {
-            if (k == 0 || left <= edge) len = (int)std::min<int64_t>(edge, left);
-            else if (left < n->chunk + edge) len = (int)(left - edge);
-        }
-        const int flags = (forced ? 1 : 0) | (current ? 2 : 0) | (raster ? 4 : 0);
+        const int len = plan[k].first;
         const size_t bytes = (size_t)len * wbytes, off = (size_t)done * wbytes;
         if (forced) {
             if (k >= 2) NET_TRY(n, cudaStreamWaitEvent(cp, n->ev_comp[b], 0));  // stage b read by chunk k-2
@@ -1680,15 +1696,12 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
         if (current && n->N)
             NET_TRY(n, cudaMemcpyAsync(n->d_current_stage, current + (size_t)done * n->N, (size_t)len * n->N * 4, in_kind, st));
         if (raster && k >= 2) NET_TRY(n, cudaStreamWaitEvent(st, n->ev_out[b], 0));  // stage b copied out
-        cudaGraphExec_t ex;
-        int rc = net_graph(n, len, flags, b, &ex);
-        if (rc) return rc;
-        NET_TRY(n, cudaGraphLaunch(ex, st));
+        NET_TRY(n, cudaGraphLaunch(plan[k].second, st));
         NET_TRY(n, cudaEventRecord(n->ev_comp[b], st));
         n->graph_launches += 1;
         n->kernel_launches += (uint64_t)((n->overlap ? 1 : 2) + (n->mon_n ? 1 : 0)) * len + 1;
         if (raster) {
-            rc = flush(b);  // bounce b last held chunk k-2
+            int rc = flush(b);  // bounce b last held chunk k-2
             if (rc) return rc;
             NET_TRY(n, cudaStreamWaitEvent(cpo, n->ev_comp[b], 0));
             char* dst = bounce_out ? (char*)n->h_io[2 + b] : (char*)raster + off;
@@ -1699,8 +1712,8 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
             if (rc) return rc;
         }
         done += len;
-        n->steps_done += len;
     }
+    n->steps_done += steps;
     for (int b = 0; b < 2; ++b) {
         int rc = flush(b);
         if (rc) return rc;

@@ -4,6 +4,7 @@ from __future__ import annotations
 import numpy as np
 
 import szsnn_b200 as sz
+from szsnn_b200.workloads import izh_network, thalamic  # noqa: F401  (shared with the benchmark)
 
 
 def if_network(n=300, n_syn=6000, max_delay=64, dyadic=True, seed=1, n_exc=None):
@@ -25,43 +26,6 @@ def if_network(n=300, n_syn=6000, max_delay=64, dyadic=True, seed=1, n_exc=None)
     return dict(n=n, src=src, tgt=tgt, w=w, d1=d1, pv=pv, v0=v0, D=max_delay)
 
 
-def izh_network(n=1000, fanout=100, seed=3, dyadic=True, half_steps=False, max_delay=20):
-    """Izhikevich pulse-coupled network shaped like the 1000-neuron benchmark
-    (800 RS / 200 FS, 100 distinct non-self targets, exc delays U{1..20},
-    inh delay 1), with parameters drawn from r ~ U(0,1)."""
-    rng = np.random.default_rng(seed)
-    ne = int(0.8 * n)
-    re = rng.uniform(0, 1, ne).astype(np.float32)
-    ri = rng.uniform(0, 1, n - ne).astype(np.float32)
-    a = np.concatenate([np.full(ne, 0.02), 0.02 + 0.08 * ri]).astype(np.float32)
-    b = np.concatenate([np.full(ne, 0.2), 0.25 - 0.05 * ri]).astype(np.float32)
-    c = np.concatenate([-65 + 15 * re ** 2, np.full(n - ne, -65.0)]).astype(np.float32)
-    d = np.concatenate([8 - 6 * re ** 2, np.full(n - ne, 2.0)]).astype(np.float32)
-    src, tgt = [], []
-    for s in range(n):
-        cand = rng.choice(n - 1, fanout, replace=False)
-        cand[cand >= s] += 1
-        src.append(np.full(fanout, s))
-        tgt.append(cand)
-    src = np.concatenate(src)
-    tgt = np.concatenate(tgt)
-    exc = src < ne
-    w = np.where(exc, 6.0, -5.0).astype(np.float32) if dyadic else np.where(exc, 6.0, -5.0).astype(np.float32)
-    d1 = np.where(exc, rng.integers(1, max_delay + 1, len(src)), 1).astype(np.uint32)
-    v0 = np.full(n, -65.0, np.float32)
-    u0 = (b * v0).astype(np.float32)
-    return dict(n=n, src=src, tgt=tgt, w=w, d1=d1, a=a, b=b, c=c, d=d, v0=v0, u0=u0, ne=ne, D=max_delay)
-
-
-def thalamic(n, ne, steps, seed=7):
-    """N(0,1)*5 to excitatory, *2 to inhibitory neurons, per step."""
-    rng = np.random.default_rng(seed)
-    x = rng.standard_normal((steps, n)).astype(np.float32)
-    x[:, :ne] *= np.float32(5.0)
-    x[:, ne:] *= np.float32(2.0)
-    return x
-
-
 def forced_schedule(n, steps, every=7, first=3):
     return [list(range(0, n, every)) if t < first else None for t in range(steps)]
 
@@ -73,3 +37,22 @@ def forced_words(sched, n_units):
         if ids is not None and len(ids):
             fw[t] = sz.ids_to_words(ids, n_units)
     return fw
+
+
+def raster_bits(raster, n):
+    """[steps][W] uint32 words -> [steps][n] bool."""
+    return np.unpackbits(raster.view(np.uint8), bitorder="little").reshape(raster.shape[0], -1)[:, :n].astype(bool)
+
+
+def rate_cv(raster, n, dt_ms):
+    """(population rate in Hz, ISI-CV of the pooled inter-spike intervals, spikes) of units 0..n-1."""
+    b = raster_bits(raster, n)
+    steps = b.shape[0]
+    rate = b.sum() / n / (steps * dt_ms * 1e-3)
+    t, i = np.nonzero(b)
+    order = np.lexsort((t, i))
+    t, i = t[order], i[order]
+    same = i[1:] == i[:-1]
+    isi = (t[1:] - t[:-1])[same].astype(np.float64)
+    cv = isi.std() / isi.mean() if isi.size > 10 else float("nan")
+    return rate, cv, int(b.sum())

@@ -21,7 +21,7 @@ Workloads:
   2. IF_curr_exp balanced network, 3200 / 800 neurons, connection probability
      0.02, w 0.25 / -2.25 nA, delays U{1..100} steps at dt 0.1 ms, 1000 Poisson
      sources at 10 Hz with fan-out probability 0.02, 10,000 steps;
-  3. the 1M IF_cond_exp benchmark network (bench.cond_config: fan-out 1000,
+  3. the 1M IF_cond_exp benchmark network (workloads.cond_config: fan-out 1000,
      delays U{1..64}, 10 % Poisson sources at 5 Hz) at 100k neurons so the
      oracle finishes in seconds, 2000 steps.
 Workloads 1 and 2 have dyadic weights, so every fp32 sum is exact whatever the
@@ -36,7 +36,8 @@ import pytest
 
 import oracle
 import szsnn_b200 as sz
-from tests.helpers import izh_network, thalamic
+from szsnn_b200.workloads import cond_config, if4000, init_state, izh_network, thalamic
+from tests.helpers import rate_cv, raster_bits
 
 pytestmark = pytest.mark.gpu
 
@@ -50,21 +51,8 @@ def ctx(built):
     c.close()
 
 
-def _bits(raster, n):
-    return np.unpackbits(raster.view(np.uint8), bitorder="little").reshape(raster.shape[0], -1)[:, :n].astype(bool)
-
-
-def _rate_cv(raster, n, dt_ms):
-    b = _bits(raster, n)
-    steps = b.shape[0]
-    rate = b.sum() / n / (steps * dt_ms * 1e-3)
-    t, i = np.nonzero(b)
-    order = np.lexsort((t, i))
-    t, i = t[order], i[order]
-    same = i[1:] == i[:-1]
-    isi = (t[1:] - t[:-1])[same].astype(np.float64)
-    cv = isi.std() / isi.mean() if isi.size > 10 else float("nan")
-    return rate, cv, int(b.sum())
+_bits = raster_bits
+_rate_cv = rate_cv
 
 
 def _run_snapshots(run, steps, get_state):
@@ -153,34 +141,9 @@ def test_izhikevich_1000(ctx):
     net.close()
 
 
-def _if_balanced(seed=11):
-    rng = np.random.default_rng(seed)
-    n, ne, p_src = 4000, 3200, 1000
-    src, tgt, w, d1 = [], [], [], []
-    for s in range(n + p_src):
-        k = rng.binomial(n, 0.02)
-        t = rng.choice(n, k, replace=False)
-        src.append(np.full(k, s))
-        tgt.append(t)
-        if s < n:
-            w.append(np.full(k, 0.25 if s < ne else -2.25, np.float32))
-            d1.append(rng.integers(1, 101, k) + 1)  # user delay U{1..100} steps, stored +1
-        else:
-            w.append(np.full(k, 0.25, np.float32))
-            d1.append(np.full(k, 1))
-    src, tgt, w, d1 = (np.concatenate(x) for x in (src, tgt, w, d1))
-    pv = sz.fold_dt(sz.if_params(v_rest=-60, cm=0.2, tau_m=20, tau_refrac=5, tau_syn_E=5, tau_syn_I=10,
-                                 v_reset=-60, v_thresh=-50), 0.1)
-    pops = [sz.Pop(sz.IF_CURR_EXP, 0, n, pv),
-            sz.Pop(sz.POISSON, n, n + p_src, np.array([10.0 * 0.1e-3], np.float32), seed=77)]
-    v0 = np.concatenate([rng.uniform(-60, -50, n), np.zeros(p_src)]).astype(np.float32)
-    fr = np.concatenate([np.full(n, 1e4), np.zeros(p_src)]).astype(np.float32)
-    csr = sz.csr_from_synapses(n + p_src, 101, src, tgt, w, d1.astype(np.uint32))
-    return n, p_src, pops, csr, [v0, None, None, fr]
-
-
 def test_if_curr_exp_balanced_4000(ctx):
-    n, p, pops, csr, st = _if_balanced()
+    w = if4000(seed=11)
+    n, p, pops, csr, st = w["n"], w["p"], w["pops"], w["csr"], w["state"]
     net = sz.Network(ctx, n, p, 101, pops, csr=csr, state=st, graph_chunk=50)
     onet = oracle.OracleNet(n, p, 101, pops, csr, state=st)
     o64 = oracle.OracleNet(n, p, 101, pops, csr, state=st, dtype=np.float64)
@@ -191,9 +154,8 @@ def test_if_curr_exp_balanced_4000(ctx):
 def test_if_cond_exp_100k(ctx):
     """The benchmark's network builder (same populations, generator blocks,
     weights, delays, Poisson rate and initial state) at 100k neurons."""
-    import bench
-    n, p, D, blocks, pops = bench.cond_config(100_000, 1000)
-    st = bench.init_state(n, p, 3)
+    n, p, D, blocks, pops = cond_config(100_000, 1000)
+    st = init_state(n, p, 3)
     net = sz.Network(ctx, n, p, D, pops, state=st, graph_chunk=50)
     net.generate(blocks, seed=31)
     csr = oracle.generate(blocks, 31, n + p, D)

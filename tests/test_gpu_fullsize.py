@@ -1,23 +1,40 @@
 """GPU: the benchmark network at its full size (1M IF_cond_exp neurons x 1000
-synapses + 100k Poisson sources x 100, delays U{1..64}), where the oracle
-cannot follow, through properties that do not depend on size:
+synapses + 100k Poisson sources x 100, delays U{1..64}), the configuration
+the headline number is quoted on.
 
-  * in fixed-point accumulation the overlapped step order (one fused launch:
-    four-unit bulk-copied update tiles, delay-1 delivery by the spiking warps,
-    delays 2..64 by the delivery blocks) and the classic order (delivery, then
-    update) give the same rasters, state, spike and event counts, bit for bit;
-  * a checkpoint taken in one order and restored into the other network
-    continues the same trajectory.
+  * against the oracle (generated on the CPU from the same seed by the same
+    algorithm, run on all host threads):
+      - fixed-point accumulation: rasters, all four state slots and the event
+        count bit for bit over 100 steps;
+      - fp32 atomic accumulation (the benchmark's mode): rasters bit-exact for
+        the first 100 steps, state within 1e-5 relative at the last snapshot
+        before the first differing step, population rate and ISI-CV within
+        1 % over 600 steps, and the membrane error against the oracle's FP64
+        twin at step 50;
+  * properties that hold at any size, in fixed point: the overlapped step
+    order (one fused launch) and the classic order (delivery, then update)
+    give the same rasters, state, spike and event counts; a checkpoint taken
+    in one order and restored into the other network continues the same
+    trajectory.
 """
+import json
+import os
+
 import numpy as np
 import pytest
 
+import oracle
 import szsnn_b200 as sz
 from szsnn_b200 import _lib as L
+from szsnn_b200.workloads import cond_config, init_state
+from tests.helpers import rate_cv
 
 pytestmark = pytest.mark.gpu
 
 STEPS = 60
+N_FULL = 1_000_000
+SEED = 1
+THREADS = os.cpu_count() or 1
 
 
 @pytest.fixture(scope="module")
@@ -27,13 +44,76 @@ def ctx(built):
     c.close()
 
 
-def _bench_net(ctx, overlap):
-    import bench
-    n, p, D, blocks, pops = bench.cond_config(1_000_000, 1000)
-    net = sz.Network(ctx, n, p, D, pops, state=bench.init_state(n, p, 1), acc_mode=L.ACC_FIXED, graph_chunk=20)
-    net.generate(blocks, seed=1)
+@pytest.fixture(scope="module")
+def full_csr():
+    """The 1M network's synapses generated on the CPU (oracle generator)."""
+    n, p, D, blocks, pops = cond_config(N_FULL, 1000)
+    return oracle.generate(blocks, SEED, n + p, D)
+
+
+def _bench_net(ctx, overlap, acc=L.ACC_FIXED, chunk=20):
+    n, p, D, blocks, pops = cond_config(N_FULL, 1000)
+    net = sz.Network(ctx, n, p, D, pops, state=init_state(n, p, SEED), acc_mode=acc, graph_chunk=chunk)
+    net.generate(blocks, seed=SEED)
     net.set_overlap(overlap)
     return net
+
+
+def _oracle_net(csr, dtype=np.float32):
+    n, p, D, blocks, pops = cond_config(N_FULL, 1000)
+    return oracle.OracleNet(n, p, D, pops, csr, state=init_state(n, p, SEED), dtype=dtype)
+
+
+def test_full_size_fixed_point_equals_oracle(ctx, full_csr):
+    net = _bench_net(ctx, True)
+    r_gpu = net.run(100)
+    on = _oracle_net(full_csr)
+    r_orc, ev = on.run(100, acc_mode=oracle.ACC_FIXED, nthreads=THREADS)
+    assert np.array_equal(r_gpu, r_orc)
+    for k in range(4):
+        assert np.array_equal(net.get_state(k), on.state[k]), f"state slot {k}"
+    assert net.stats()["events"] == ev
+    assert ev > 1_000_000 and int(np.unpackbits(r_orc.view(np.uint8)).sum()) > 10_000
+    net.close()
+
+
+def test_full_size_float_matches_oracle(ctx, full_csr):
+    steps, snap = 600, 50
+    n, p = N_FULL, N_FULL // 10
+    net = _bench_net(ctx, True, acc=L.ACC_FLOAT, chunk=50)
+    on = _oracle_net(full_csr)
+    parts_g, parts_o, snaps_g, snaps_o = [], [], {}, {}
+    for t in range(0, steps, snap):
+        parts_g.append(net.run(snap))
+        parts_o.append(on.run(snap, nthreads=THREADS)[0])
+        snaps_g[t + snap] = [net.get_state(k)[:n] for k in range(4)]
+        snaps_o[t + snap] = [on.state[k][:n].copy() for k in range(4)]
+    net.close()
+    r_gpu, r_orc = np.concatenate(parts_g), np.concatenate(parts_o)
+    assert np.array_equal(r_gpu[:100], r_orc[:100])
+    diff = np.nonzero(np.any(r_gpu != r_orc, axis=1))[0]
+    flip = int(diff[0]) if diff.size else steps
+    snap_t = max(t for t in snaps_g if t <= flip)
+    for k in range(4):
+        a, b = snaps_g[snap_t][k].astype(np.float64), snaps_o[snap_t][k].astype(np.float64)
+        scale = max(np.abs(b).max(), 1e-30)
+        assert np.allclose(a, b, rtol=1e-5, atol=1e-5 * scale), (k, snap_t)
+    rg, cg, ng = rate_cv(r_gpu, n, 0.1)
+    ro, co, no = rate_cv(r_orc, n, 0.1)
+    assert no > 100_000, no
+    assert abs(rg - ro) <= 0.01 * ro, (rg, ro)
+    assert abs(cg - co) <= 0.01 * co, (cg, co)
+    # membrane error against the FP64 twin at step 50 (single-threaded: its
+    # double accumulation has no atomic form)
+    o64 = _oracle_net(full_csr, np.float64)
+    r64, _ = o64.run(snap, nthreads=1)
+    v64 = o64.state[0][:n]
+    err = float(np.max(np.abs(snaps_g[snap][0].astype(np.float64) - v64)) / np.abs(v64).max())
+    print(json.dumps({"workload": "if_cond_exp-1M", "steps": steps, "first_flip_vs_fp32_oracle": flip,
+                      "rate_hz": [rg, ro], "isi_cv": [cg, co], "spikes": [ng, no],
+                      "rasters_equal_fp64_first_50": bool(np.array_equal(r_gpu[:snap], r64)),
+                      "v_rel_err_vs_fp64_step50": err}))
+    assert err <= 1e-4, err
 
 
 def test_full_size_orders_agree_and_checkpoint_continues(ctx):

@@ -68,8 +68,9 @@ def test_reference_arm_other_ranks_do_nothing(capsys):
 
 def test_reference_arm_reports_the_steps_it_was_given(capsys):
     """The reference arm's line carries the K timed and W warm-up steps of its
-    command line, each step S = ceil(2000 / K) simulation steps of the CPU
-    sample, and its value is the sample's events over the timed steps."""
+    command line, each step S = ceil(2000 / K) simulation steps of the
+    network the port runs, and its value is that network's events over the
+    timed steps."""
     import json
     sys.path.insert(0, ROOT)
     import bench
@@ -77,6 +78,6 @@ def test_reference_arm_reports_the_steps_it_was_given(capsys):
     bench.run_reference(args, rank=0)
     line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["steps"] == 3 and line["warmup"] == 4
-    assert line["config"]["sim_steps_per_step"] == 667
+    assert line["sim_steps_per_step"] == 667
     assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
