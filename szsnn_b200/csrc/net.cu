@@ -336,17 +336,40 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ NetDe
     propagate_grouped<G>(nd, k_off, m_lo, pf, blockIdx.x, gridDim.x);
 }
 
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// 8-byte asynchronous copy global -> shared (no register holds the data in
+// flight); completed by cp_async_wait_all in the issuing thread
+__device__ __forceinline__ void cp_async8(void* dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(smem_addr(dst)), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Synapses in flight per lane of a delivery warp, and the shared-memory
+// window that holds them: 32 * FAR_WPL int2 per warp
+#define FAR_WPL 12
+__host__ __device__ __forceinline__ size_t far_window_bytes(int block_threads)
+{
+    return (size_t)(block_threads / 32) * 32 * FAR_WPL * sizeof(int2);
+}
+
 // Warp-flattened delivery: lanes 0..IPW-1 each resolve one (delay, spike)
 // work item to its bucket segment; the warp then walks the concatenation of
-// those segments 32 synapses at a time (owner segment found by a binary
-// search over the lanes' exclusive offsets with shuffles), UNR loads in
-// flight per lane before their atomics (8 in the delivery kernel of its own,
-// 4 inside the step kernel, whose register budget is shared with the update).
-template <int IPW, int UNR>
+// those segments in windows of 32 * FAR_WPL synapses.  Each item lane issues
+// asynchronous 8-byte copies of its segment's part of the window into the
+// warp's shared-memory slice and waits for them; after a warp barrier every
+// lane delivers FAR_WPL entries of the window: one memory round trip per
+// window rather than one per few loads, with no registers holding the loads
+// in flight.
+// Dynamic shared memory: far_window_bytes(blockDim.x).
+template <int IPW>
 __device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int m_lo, uint32_t pf, int blk, int nblk)
 {
     __shared__ uint32_t s_pre[1025];
     __shared__ unsigned long long s_ev;
+    extern __shared__ __align__(128) unsigned char upd_smem[];
     const long long t = *nd.clock + k_off;
     const int D = nd.D, R = D + 1;
     propagate_prologue(nd, t, m_lo, pf, s_pre, &s_ev, blk == 0);
@@ -356,6 +379,7 @@ __device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int 
     const int64_t gw = ((int64_t)blk * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)nblk * blockDim.x) >> 5;
     const int2* __restrict__ syn = nd.syn;
+    int2* const win = reinterpret_cast<int2*>(upd_smem) + (size_t)(threadIdx.x >> 5) * 32 * FAR_WPL;
     uint32_t ev = 0;
     for (int64_t base = gw * IPW; base < (int64_t)total; base += nw * IPW) {
         const int64_t item = base + lane;
@@ -389,36 +413,30 @@ __device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int 
         }
         const uint32_t excl = incl - len;
         const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
-        for (uint32_t k0 = 0; k0 < tot; k0 += 32 * UNR) {
-            int2 sw[UNR];
-            bool ok[UNR];
+        // window [k0, k0 + W) of the concatenation: each item lane copies the
+        // part of its own segment inside the window to its place in the
+        // warp's slice, waits for its copies, and after a warp barrier every
+        // lane delivers W / 32 entries of the window
+        constexpr uint32_t W = 32 * FAR_WPL;
+        for (uint32_t k0 = 0; k0 < tot; k0 += W) {
+            const uint32_t j0 = k0 > excl ? k0 - excl : 0u;
+            const uint32_t j1 = min(len, k0 + W - min(k0 + W, excl));
+            for (uint32_t j = j0; j < j1; ++j) cp_async8(&win[excl + j - k0], &syn[a + j]);
+            cp_async_wait_all();
+            __syncwarp();
 #pragma unroll
-            for (int u = 0; u < UNR; ++u) {
-                const uint32_t k = k0 + 32u * u + lane;
-                ok[u] = k < tot;
-                int owner = 0;  // last lane whose segment starts at or before k
-#pragma unroll
-                for (int st = 16; st >= 1; st >>= 1) {
-                    const int cand = owner + st;
-                    const uint32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
-                    if (cand < 32 && ex <= k) owner = cand;
-                }
-                const unsigned long long oa = __shfl_sync(0xffffffffu, a, owner);
-                const uint32_t oex = __shfl_sync(0xffffffffu, excl, owner);
-                sw[u] = ok[u] ? __ldg(&syn[oa + (k - oex)]) : make_int2(0, 0);
-            }
-#pragma unroll
-            for (int u = 0; u < UNR; ++u)
-                if (ok[u]) deliver(nd, buf, sw[u], ev);
+            for (int u = 0; u < FAR_WPL; ++u)
+                if (k0 + 32u * u + lane < tot) deliver(nd, buf, win[32 * u + lane], ev);
+            __syncwarp();
         }
     }
     propagate_epilogue(nd, t, pf, ev, &s_ev);
 }
 
 template <int IPW>
-__global__ void __launch_bounds__(256) k_propagate_flat(const __grid_constant__ NetDev nd, int k_off, int m_lo, uint32_t pf)
+__global__ void __launch_bounds__(256, 4) k_propagate_flat(const __grid_constant__ NetDev nd, int k_off, int m_lo, uint32_t pf)
 {
-    propagate_flat<IPW, 8>(nd, k_off, m_lo, pf, blockIdx.x, gridDim.x);
+    propagate_flat<IPW>(nd, k_off, m_lo, pf, blockIdx.x, gridDim.x);
 }
 
 // last population with begin <= id, or -1 (ranges sorted and disjoint)
@@ -565,8 +583,6 @@ __device__ __forceinline__ TileSmem tile_smem(unsigned char* base, uint32_t T, b
     m.fi = m.fe + T;
     return m;
 }
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
@@ -870,7 +886,7 @@ __global__ void __launch_bounds__(UPD_MAX_BLOCK, UPD_MIN_BLOCKS) k_step(const __
 {
     if ((int)blockIdx.x < far_blocks) {  // G > 0: grouped delivery, G lanes per bucket; G < 0: flattened, -G items per warp
         if constexpr (G > 0) propagate_grouped<G>(nd, k_off + 1, 2, PF_PENDING, blockIdx.x, far_blocks);
-        else propagate_flat<-G, 4>(nd, k_off + 1, 2, PF_PENDING, blockIdx.x, far_blocks);
+        else propagate_flat<-G>(nd, k_off + 1, 2, PF_PENDING, blockIdx.x, far_blocks);
         return;
     }
     update_body(nd, k_off, blockIdx.x - far_blocks, forced, current, out_words);
@@ -1055,10 +1071,11 @@ cudaError_t launch_propagate(szsnn_net* n, const NetDev& d, int k_off, int m_lo,
 {
     int blocks = n->prop_blocks > 0 ? n->prop_blocks : num_sms(n->ctx) * 16;
     if (n->prop_mode == 1) {
+        const size_t sm = far_window_bytes(256);
         switch (n->prop_group) {
-        case 8: k_propagate_flat<8><<<blocks, 256, 0, st>>>(d, k_off, m_lo, pf); break;
-        case 16: k_propagate_flat<16><<<blocks, 256, 0, st>>>(d, k_off, m_lo, pf); break;
-        default: k_propagate_flat<32><<<blocks, 256, 0, st>>>(d, k_off, m_lo, pf); break;
+        case 8: k_propagate_flat<8><<<blocks, 256, sm, st>>>(d, k_off, m_lo, pf); break;
+        case 16: k_propagate_flat<16><<<blocks, 256, sm, st>>>(d, k_off, m_lo, pf); break;
+        default: k_propagate_flat<32><<<blocks, 256, sm, st>>>(d, k_off, m_lo, pf); break;
         }
         return cudaGetLastError();
     }
@@ -1109,13 +1126,15 @@ cudaError_t fill_blk_pop(szsnn_net* n)
 }
 
 // dynamic shared memory of an update launch: an inline tile when any block
-// of the launch runs one; the kernel's limit raised when that is above 48 KB
+// of the launch runs one, at least `floor` bytes (the delivery blocks' copy
+// windows in a fused step); the kernel's limit raised when above 48 KB
 template <class K>
-cudaError_t update_smem(const NetDev& d, int bs, K kernel, size_t* bytes)
+cudaError_t update_smem(const NetDev& d, int bs, K kernel, size_t* bytes, size_t floor = 0)
 {
     bool any = false;
     for (int i = 0; i < INLINE_POPS; ++i) any = any || d.ib_hi[i] > d.ib_lo[i];
     *bytes = any ? tile_smem_bytes((int64_t)d.upt * bs, d.acc_mode == SZSNN_ACC_FIXED) : 0;
+    *bytes = std::max(*bytes, floor);
     if (*bytes > 48 * 1024)
         return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*bytes);
     return cudaSuccess;
@@ -1153,9 +1172,10 @@ cudaError_t launch_step(szsnn_net* n, const NetDev& d, int k_off, const uint32_t
     const dim3 grid((unsigned)blocks);
     size_t smem = 0;
     cudaError_t e = cudaSuccess;
+    const size_t win = (far > 0 && n->prop_mode == 1) ? far_window_bytes(bs) : 0;
 #define SZ_STEP(G)                                                         \
     do {                                                                  \
-        e = update_smem(d, bs, k_step<G>, &smem);                         \
+        e = update_smem(d, bs, k_step<G>, &smem, win);                    \
         if (e == cudaSuccess) k_step<G><<<grid, bs, smem, st>>>(d, k_off, far, forced, cur, words); \
     } while (0)
     if (n->prop_mode == 1) {

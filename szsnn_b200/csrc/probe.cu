@@ -7,8 +7,9 @@
 // either part; these two probes measure what does, on the device at hand:
 //
 //  * L2 copy bandwidth: a float4 grid-stride copy between two 16 MB buffers
-//    (both resident in L2 after the first pass), read + write bytes per
-//    second;
+//    (both resident in L2), repeated `passes` times inside one launch so
+//    launch gaps do not count; loads bypass L1 (ld.global.cg), so every pass
+//    moves its bytes between L2 and the SMs; read + write bytes per second;
 //  * random reductions: `red.global.add.f32` at hashed addresses into two
 //    arrays of n_targets floats (the exc / inh accumulators of an n-neuron
 //    network), reductions per second.  No loads feed them, so this is the
@@ -20,10 +21,12 @@
 
 namespace {
 
-__global__ void __launch_bounds__(256) k_probe_copy(const float4* __restrict__ a, float4* __restrict__ b, int64_t n4)
+__global__ void __launch_bounds__(256) k_probe_copy(const float4* __restrict__ a, float4* __restrict__ b, int64_t n4,
+                                                    int passes)
 {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x)
-        b[i] = a[i];
+    for (int r = 0; r < passes; ++r)
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x)
+            b[i] = __ldcg(&a[i]);
 }
 
 // 32-bit mix (the finaliser of MurmurHash3), for probe addresses only
@@ -83,18 +86,19 @@ extern "C" int szsnn_probe_peaks(szsnn_ctx* ctx, int64_t n_targets, szsnn_peaks*
     P_TRY(cudaEventCreate(&e0));
     P_TRY(cudaEventCreate(&e1));
 
-    // L2-resident copy: 8 blocks of 256 threads per SM, 3 warm-up passes, 50 timed
-    const int cgrid = sms * 8, creps = 50;
-    for (int r = 0; r < 3; ++r) k_probe_copy<<<cgrid, 256, 0, st>>>(a, b, n4);
+    // L2-resident copy: 8 blocks of 256 threads per SM, 16 passes per launch,
+    // 2 warm-up launches, 5 timed
+    const int cgrid = sms * 8, passes = 16, creps = 5;
+    for (int r = 0; r < 2; ++r) k_probe_copy<<<cgrid, 256, 0, st>>>(a, b, n4, passes);
     P_TRY(cudaGetLastError());
     P_TRY(cudaEventRecord(e0, st));
-    for (int r = 0; r < creps; ++r) k_probe_copy<<<cgrid, 256, 0, st>>>(r & 1 ? b : a, r & 1 ? a : b, n4);
+    for (int r = 0; r < creps; ++r) k_probe_copy<<<cgrid, 256, 0, st>>>(r & 1 ? b : a, r & 1 ? a : b, n4, passes);
     P_TRY(cudaGetLastError());
     P_TRY(cudaEventRecord(e1, st));
     P_TRY(cudaEventSynchronize(e1));
     float ms = 0;
     P_TRY(cudaEventElapsedTime(&ms, e0, e1));
-    out->l2_copy_gbs = (double)creps * 2.0 * (double)copy_bytes / (ms * 1e-3) / 1e9;
+    out->l2_copy_gbs = (double)creps * passes * 2.0 * (double)copy_bytes / (ms * 1e-3) / 1e9;
     out->l2_copy_bytes = 2 * copy_bytes;
 
     // random reductions into 2 * n_targets floats

@@ -10,7 +10,8 @@ the headline number is quoted on.
         the first 100 steps, state within 1e-5 relative at the last snapshot
         before the first differing step, population rate and ISI-CV within
         1 % over 600 steps, and the membrane error against the oracle's FP64
-        twin at step 50;
+        twin at the last step before the first spike that differs from it
+        (within the first 50 steps);
   * properties that hold at any size, in fixed point: the overlapped step
     order (one fused launch) and the classic order (delivery, then update)
     give the same rasters, state, spike and event counts; a checkpoint taken
@@ -103,17 +104,34 @@ def test_full_size_float_matches_oracle(ctx, full_csr):
     assert no > 100_000, no
     assert abs(rg - ro) <= 0.01 * ro, (rg, ro)
     assert abs(cg - co) <= 0.01 * co, (cg, co)
-    # membrane error against the FP64 twin at step 50 (single-threaded: its
-    # double accumulation has no atomic form)
-    o64 = _oracle_net(full_csr, np.float64)
-    r64, _ = o64.run(snap, nthreads=1)
-    v64 = o64.state[0][:n]
-    err = float(np.max(np.abs(snaps_g[snap][0].astype(np.float64) - v64)) / np.abs(v64).max())
     print(json.dumps({"workload": "if_cond_exp-1M", "steps": steps, "first_flip_vs_fp32_oracle": flip,
-                      "rate_hz": [rg, ro], "isi_cv": [cg, co], "spikes": [ng, no],
-                      "rasters_equal_fp64_first_50": bool(np.array_equal(r_gpu[:snap], r64)),
-                      "v_rel_err_vs_fp64_step50": err}))
-    assert err <= 1e-4, err
+                      "rate_hz": [rg, ro], "isi_cv": [cg, co], "spikes": [ng, no]}))
+
+
+def test_full_size_float_against_fp64(ctx, full_csr):
+    """Membrane error of the fp32 GPU run against the oracle's FP64 twin (the
+    same update equations in double), step by step over the first 50 steps:
+    max |dv| / max |v| at the last step before the first step whose spikes
+    differ (a near-threshold unit that spikes in one run and not the other
+    shifts its v by the reset), or at step 50 when none does."""
+    n = N_FULL
+    net = _bench_net(ctx, True, acc=L.ACC_FLOAT, chunk=50)
+    o64 = _oracle_net(full_csr, np.float64)  # single-threaded: its double accumulation has no atomic form
+    last_err, flip = None, None
+    for t in range(50):
+        words = net.step()
+        r64, _ = o64.run(1, nthreads=1)
+        if not np.array_equal(words, r64[0]):
+            flip = t
+            break
+        v = net.get_state(0)[:n].astype(np.float64)
+        v64 = o64.state[0][:n]
+        last_err = float(np.max(np.abs(v - v64)) / np.abs(v64).max())
+    net.close()
+    print(json.dumps({"workload": "if_cond_exp-1M", "first_flip_vs_fp64": flip if flip is not None else ">=50",
+                      "v_rel_err_vs_fp64_before_flip": last_err}))
+    assert last_err is not None, "spikes differ from the FP64 twin at step 0"
+    assert last_err <= 1e-4, last_err
 
 
 def test_full_size_orders_agree_and_checkpoint_continues(ctx):
