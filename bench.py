@@ -79,8 +79,9 @@ def parse(argv=None):
                     help="keep the default launch shape instead of autotuning after the warm-up")
     ap.add_argument("--tune-after", type=int, default=3000, help="steps simulated before the tuner's replays")
     ap.add_argument("--shape", default=None,
-                    help="fixed launch shape 'order,mode,group,blocks,update_block' (order: overlapped|classic) "
-                         "instead of the tuner")
+                    help="fixed launch shape 'order,mode,group,blocks,update_block[,tiles,per_sm]' (order: "
+                         "overlapped|classic; tiles 0 block tiles, 1 persistent warp tiles with per_sm update "
+                         "blocks per SM) instead of the tuner")
     ap.add_argument("--e2e-steps", type=int, default=2000)
     ap.add_argument("--profile-steps", type=int, default=200)
     ap.add_argument("--cpu-neurons", type=int, default=None,
@@ -539,11 +540,14 @@ def main():
     ctx.sync()
     tuning = None
     if args.shape:
-        order, mode, group, blocks_, ub = args.shape.split(",")
+        f = args.shape.split(",")
+        order, mode, group, blocks_, ub = f[:5]
+        tiles, per_sm = (int(f[5]), int(f[6])) if len(f) >= 7 else (0, 0)
         net.set_overlap(order == "overlapped")
         net.set_tuning(int(mode), int(group), int(blocks_), int(ub))
+        net.set_update_tiles(tiles, per_sm)
         tuning = {"overlap": order == "overlapped", "mode": int(mode), "group": int(group), "blocks": int(blocks_),
-                  "update_block": int(ub), "source": "--shape"}
+                  "update_block": int(ub), "update_tiles": tiles, "update_per_sm": per_sm, "source": "--shape"}
     elif args.tune:  # past the start-up transient (v(0) ~ U(-60,-50) fires a first volley)
         from szsnn_b200.autotune import tune
         net.run_device(max(0, args.tune_after - W * S))

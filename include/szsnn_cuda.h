@@ -343,6 +343,13 @@ int szsnn_net_timing(szsnn_net* net, double* propagate_ms, double* update_ms, do
  * warp (8/16/32); propagate grid blocks (0 = 16 per SM); update block size
  * (threads, a multiple of 32 in 32..256; each thread updates 4 units) */
 int szsnn_net_set_tuning(szsnn_net* net, int propagate_mode, int group, int propagate_blocks, int update_block);
+/* Update tiles: mode 0 = one tile per update block, a new block per tile each
+ * step; mode 1 = persistent warp tiles: blocks_per_sm update blocks per SM
+ * (0 = 2), each warp streaming 128-unit tiles through a two-stage ring of
+ * bulk copies in shared memory and writing them back with bulk stores.  Mode
+ * 1 applies to networks of at most four populations; others keep mode 0.
+ * Results are identical in both modes. */
+int szsnn_net_set_update_tiles(szsnn_net* net, int mode, int blocks_per_sm);
 /* Step order.  1 (default): overlapped -- input buffers double-buffered by
  * step parity, delivery of delays >= 2 into step t+1 runs in the same launch
  * as update(t), and update(t) delivers the delay-1 bucket of its own

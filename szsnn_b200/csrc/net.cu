@@ -87,6 +87,7 @@ struct NetDev {
     int32_t upt;                           // units per update thread (1..UPD_UPT)
     int32_t ib_lo[INLINE_POPS], ib_hi[INLINE_POPS];  // update blocks [lo, hi) lying inside slot i (empty: none)
     PopDev ipop[INLINE_POPS];              // populations with shared parameters, by value in the kernel parameters
+    uint32_t warp_tiles;                   // 1: persistent warp-tile update (update_warp_tiles)
 };
 
 struct szsnn_net {
@@ -138,6 +139,7 @@ struct szsnn_net {
     int64_t steps_done = 0;
     uint64_t graph_launches = 0, kernel_launches = 0;
     int prop_mode = 0, prop_group = 16, prop_blocks = 0, upd_block = 256;
+    int upd_tiles = 0, upd_per_sm = 0;   // update tiles: 0 block tiles, 1 persistent warp tiles (blocks per SM)
     double t_prop_ms = 0, t_upd_ms = 0, t_total_ms = 0;
     cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;  // around the last szsnn_net_run*
     bool run_timed = false;
@@ -869,10 +871,304 @@ __device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk
     }
 }
 
-__global__ void __launch_bounds__(UPD_MAX_BLOCK, UPD_MIN_BLOCKS) k_update(const __grid_constant__ NetDev nd, int k_off, const uint32_t* __restrict__ forced,
-                                                const float* __restrict__ current, uint32_t* __restrict__ out_words)
+// ---- persistent warp tiles
+//
+// Each warp of the update grid streams warp tiles of WT = 128 consecutive
+// units (four raster words: lane l handles units 32 j + l, j = 0..3) through
+// a two-stage ring in its own slice of shared memory: while it updates tile
+// k from one stage, the bulk copies of its next tile (k + number of update
+// warps) fill the other.  A tile lying inside one population of the
+// parameter table is updated in place in shared memory and written back
+// with bulk stores (state and the cleared inputs); other tiles (population
+// boundaries) run the generic per-unit update from global memory.  No block
+// barrier is involved: a warp that waits on its spikes' delay-1 deliveries
+// holds up only itself, and the warps of a block drift apart freely.
+// Dynamic shared memory per warp: wt_region_bytes (two stages, two mbarriers).
+#define WT 128
+__host__ __device__ __forceinline__ constexpr uint32_t wt_stage_bytes(bool fixed) { return WT * (16u + (fixed ? 16u : 8u)); }
+__host__ __device__ __forceinline__ size_t wt_region_bytes(bool fixed) { return 2 * (size_t)wt_stage_bytes(fixed) + 16; }
+
+// arrays of a stage: st0..st3 (WT floats each), then the exc / inh inputs
+// (WT floats or WT int64 each)
+__device__ __forceinline__ float* wt_st(unsigned char* stage, int k) { return reinterpret_cast<float*>(stage) + k * WT; }
+__device__ __forceinline__ float* wt_ie(unsigned char* stage) { return reinterpret_cast<float*>(stage) + 4 * WT; }
+__device__ __forceinline__ float* wt_ii(unsigned char* stage) { return reinterpret_cast<float*>(stage) + 5 * WT; }
+__device__ __forceinline__ long long* wt_fe(unsigned char* stage) { return reinterpret_cast<long long*>(stage + 16 * WT); }
+__device__ __forceinline__ long long* wt_fi(unsigned char* stage) { return reinterpret_cast<long long*>(stage + 24 * WT); }
+
+// slot of the parameter table whose population holds units [u0, u0 + WT) of
+// the network, or -1
+__device__ __forceinline__ int wt_slot(const NetDev& nd, int64_t u0)
 {
-    update_body(nd, k_off, blockIdx.x, forced, current, out_words);
+    const int64_t u1 = min(u0 + (int64_t)WT, nd.U);
+#pragma unroll
+    for (int i = 0; i < INLINE_POPS; ++i)
+        if (nd.ipop[i].end > nd.ipop[i].begin && u0 >= nd.ipop[i].begin && u1 <= nd.ipop[i].end) return i;
+    return -1;
+}
+
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                 :: "l"(dst), "r"(smem_addr(src)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// the issuing thread's bulk stores have read their shared-memory sources
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+{
+    for (int i = 0; i < (1 << 20); ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// bulk copies of the tile at u0 (model MODEL) into a stage, completing on bar
+// (one thread); Poisson tiles read nothing
+template <int MODEL, bool FIXED>
+__device__ __forceinline__ void wt_issue(const NetDev& nd, const InBuf& inb, int64_t u0, unsigned char* sm,
+                                         uint64_t* bar)
+{
+    if (MODEL == SZSNN_POISSON) return;
+    const int64_t n = min((int64_t)WT, nd.U - u0);
+    const uint32_t b4 = (uint32_t)((n * 4 + 15) & ~(int64_t)15);
+    const uint32_t b8 = (uint32_t)((n * 8 + 15) & ~(int64_t)15);
+    const int nst = MODEL == SZSNN_IZHIKEVICH ? 2 : 4;
+    const uint32_t total = (uint32_t)nst * b4 + 2u * (FIXED ? b8 : b4);
+    asm volatile("{\n .reg .b64 s;\n mbarrier.arrive.expect_tx.shared::cta.b64 s, [%0], %1;\n}"
+                 :: "r"(smem_addr(bar)), "r"(total) : "memory");
+    float* const gst[4] = {nd.st0, nd.st1, nd.st2, nd.st3};
+    for (int k = 0; k < nst; ++k) bulk_load(wt_st(sm, k), gst[k] + u0, b4, bar);
+    if (FIXED) {
+        bulk_load(wt_fe(sm), inb.fe + u0, b8, bar);
+        bulk_load(wt_fi(sm), inb.fi + u0, b8, bar);
+    } else {
+        bulk_load(wt_ie(sm), inb.e + u0, b4, bar);
+        bulk_load(wt_ii(sm), inb.i + u0, b4, bar);
+    }
+}
+
+// issue for the tile at u0 in slot `slot` (>= 0); returns whether copies were issued
+template <bool FIXED>
+__device__ __forceinline__ bool wt_issue_slot(const NetDev& nd, int slot, const InBuf& inb, int64_t u0,
+                                              unsigned char* sm, uint64_t* bar)
+{
+    switch (nd.ipop[slot].model) {
+    case SZSNN_IF_CURR_EXP: wt_issue<SZSNN_IF_CURR_EXP, FIXED>(nd, inb, u0, sm, bar); return true;
+    case SZSNN_IF_COND_EXP: wt_issue<SZSNN_IF_COND_EXP, FIXED>(nd, inb, u0, sm, bar); return true;
+    case SZSNN_IZHIKEVICH: wt_issue<SZSNN_IZHIKEVICH, FIXED>(nd, inb, u0, sm, bar); return true;
+    default: return false;
+    }
+}
+
+// Update the tile at u0 in place in its stage (slot PI, model MODEL), each
+// 32-unit sub-tile ending in the spike epilogue; then the stage's state and
+// cleared inputs go back to global memory by bulk stores issued by lane 0.
+template <int MODEL, bool FIXED, int PI>
+__device__ __forceinline__ void wt_run(const NetDev& nd, const InBuf& inb, unsigned char* sm, int64_t u0, long long t,
+                                       bool ok, const uint32_t* __restrict__ forced,
+                                       const float* __restrict__ current, uint32_t* __restrict__ out_words)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const PopDev& P = nd.ipop[PI];
+    const SharedParams sp{P.p};
+#pragma unroll 1
+    for (int j = 0; j < WT / 32; ++j) {
+        const uint32_t u = 32u * j + lane;
+        const int64_t id = u0 + u;
+        bool spk = false;
+        if (ok && id < nd.U) {
+            const bool f = forced ? ((forced[id >> 5] >> (id & 31)) & 1u) != 0u : false;
+            if (MODEL == SZSNN_POISSON) {
+                spk = sz_poisson_fires(P.seed, id - P.begin, t, P.p[0]) || f;
+            } else {
+                float v = wt_st(sm, 0)[u], g1 = wt_st(sm, 1)[u], g2 = 0.0f, fr = 0.0f, in_e, in_i;
+                if (MODEL != SZSNN_IZHIKEVICH) { g2 = wt_st(sm, 2)[u]; fr = wt_st(sm, 3)[u]; }
+                if (FIXED) {
+                    in_e = __ll2float_rn(wt_fe(sm)[u]) * (1.0f / 4294967296.0f);
+                    in_i = __ll2float_rn(wt_fi(sm)[u]) * (1.0f / 4294967296.0f);
+                    wt_fe(sm)[u] = 0;
+                    wt_fi(sm)[u] = 0;
+                } else {
+                    in_e = wt_ie(sm)[u];
+                    in_i = wt_ii(sm)[u];
+                    wt_ie(sm)[u] = 0.0f;
+                    wt_ii(sm)[u] = 0.0f;
+                }
+                const float i_ext = current ? current[id] : 0.0f;
+                if (nd.dbg_in_e) { nd.dbg_in_e[id] = in_e; nd.dbg_in_i[id] = in_i; }
+                if (MODEL == SZSNN_IF_CURR_EXP) spk = sz_if_curr_exp(sp, v, g1, g2, fr, in_e, in_i, i_ext, f, sp(12), sp(13));
+                else if (MODEL == SZSNN_IF_COND_EXP) spk = sz_if_cond_exp(sp, v, g1, g2, fr, in_e, in_i, i_ext, f, sp(12), sp(13));
+                else spk = sz_izhikevich(sp, v, g1, in_e, in_i, i_ext, f, (P.flags & SZSNN_POP_IZH_HALF_STEPS) != 0);
+                wt_st(sm, 0)[u] = v;
+                wt_st(sm, 1)[u] = g1;
+                if (MODEL != SZSNN_IZHIKEVICH) { wt_st(sm, 2)[u] = g2; wt_st(sm, 3)[u] = fr; }
+            }
+        }
+        __syncwarp();
+        update_spikes(nd, t, id, spk, lane, out_words);
+    }
+    if (MODEL == SZSNN_POISSON || !ok) return;
+    // the lanes' shared-memory writes become visible to the bulk copy engine
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) {
+        const int64_t n = min((int64_t)WT, nd.U - u0);
+        const uint32_t b4 = (uint32_t)((n * 4 + 15) & ~(int64_t)15);
+        const uint32_t b8 = (uint32_t)((n * 8 + 15) & ~(int64_t)15);
+        const int nst = MODEL == SZSNN_IZHIKEVICH ? 2 : 4;
+        float* const gst[4] = {nd.st0, nd.st1, nd.st2, nd.st3};
+        for (int k = 0; k < nst; ++k) bulk_store(gst[k] + u0, wt_st(sm, k), b4);
+        if (FIXED) {
+            bulk_store(inb.fe + u0, wt_fe(sm), b8);
+            bulk_store(inb.fi + u0, wt_fi(sm), b8);
+        } else {
+            bulk_store(inb.e + u0, wt_ie(sm), b4);
+            bulk_store(inb.i + u0, wt_ii(sm), b4);
+        }
+        bulk_commit();
+    }
+}
+
+template <bool FIXED, int PI>
+__device__ __forceinline__ void wt_run_pop(const NetDev& nd, const InBuf& inb, unsigned char* sm, int64_t u0, long long t,
+                                           bool ok, const uint32_t* __restrict__ forced,
+                                           const float* __restrict__ current, uint32_t* __restrict__ out_words)
+{
+    switch (nd.ipop[PI].model) {
+    case SZSNN_IF_CURR_EXP: wt_run<SZSNN_IF_CURR_EXP, FIXED, PI>(nd, inb, sm, u0, t, ok, forced, current, out_words); break;
+    case SZSNN_IF_COND_EXP: wt_run<SZSNN_IF_COND_EXP, FIXED, PI>(nd, inb, sm, u0, t, ok, forced, current, out_words); break;
+    case SZSNN_IZHIKEVICH: wt_run<SZSNN_IZHIKEVICH, FIXED, PI>(nd, inb, sm, u0, t, ok, forced, current, out_words); break;
+    default: wt_run<SZSNN_POISSON, FIXED, PI>(nd, inb, sm, u0, t, ok, forced, current, out_words); break;
+    }
+}
+
+template <bool FIXED>
+__device__ __forceinline__ void wt_run_slot(const NetDev& nd, int slot, const InBuf& inb, unsigned char* sm, int64_t u0,
+                                            long long t, bool ok, const uint32_t* __restrict__ forced,
+                                            const float* __restrict__ current, uint32_t* __restrict__ out_words)
+{
+    static_assert(INLINE_POPS == 4, "one case per parameter-table slot");
+    switch (slot) {
+    case 0: wt_run_pop<FIXED, 0>(nd, inb, sm, u0, t, ok, forced, current, out_words); break;
+    case 1: wt_run_pop<FIXED, 1>(nd, inb, sm, u0, t, ok, forced, current, out_words); break;
+    case 2: wt_run_pop<FIXED, 2>(nd, inb, sm, u0, t, ok, forced, current, out_words); break;
+    default: wt_run_pop<FIXED, 3>(nd, inb, sm, u0, t, ok, forced, current, out_words); break;
+    }
+}
+
+// The persistent update of one warp: warp gw of nw update warps takes warp
+// tiles gw, gw + nw, ... (see the section comment).  Every bulk copy issued
+// is waited for (bounded; device error 7 when a wait runs out, after which
+// the warp stops taking tiles), and lane 0 waits for its bulk stores to have
+// read their sources before the warp leaves.
+template <bool FIXED>
+__device__ __forceinline__ void update_warp_tiles(const NetDev& nd, int k_off, int gw, int nw,
+                                                  const uint32_t* __restrict__ forced,
+                                                  const float* __restrict__ current, uint32_t* __restrict__ out_words)
+{
+    extern __shared__ __align__(128) unsigned char upd_smem[];
+    const uint32_t lane = threadIdx.x & 31;
+    unsigned char* reg = upd_smem + (size_t)(threadIdx.x >> 5) * wt_region_bytes(FIXED);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(reg + 2 * wt_stage_bytes(FIXED));
+    constexpr uint32_t SB = wt_stage_bytes(FIXED);
+    const long long t = *nd.clock + k_off;
+    const InBuf inb = in_buf_k(nd, k_off);
+    const int nwt = (int)((nd.U + WT - 1) / WT);  // units < 2^31
+    if (lane == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    uint32_t ph = 0;        // bit s: parity of the next wait on stage s
+    uint32_t pending = 0;   // lane 0: bit s set while stage s has copies not yet waited for
+    if (lane == 0 && gw < nwt) {
+        const int sl = wt_slot(nd, (int64_t)gw * WT);
+        if (sl >= 0 && wt_issue_slot<FIXED>(nd, sl, inb, (int64_t)gw * WT, reg, &bar[0])) pending |= 1u;
+    }
+    int k = 0;
+    for (int wt = gw; wt < nwt; wt += nw, ++k) {
+        const int s = k & 1;
+        const int nxt = wt + nw;
+        if (lane == 0) {
+            bulk_wait_read();  // the stores of the previous tile (stage s ^ 1) have read their sources
+            if (nxt < nwt) {
+                const int sl = wt_slot(nd, (int64_t)nxt * WT);
+                if (sl >= 0 && wt_issue_slot<FIXED>(nd, sl, inb, (int64_t)nxt * WT, reg + (s ^ 1) * SB, &bar[s ^ 1]))
+                    pending |= 1u << (s ^ 1);
+            }
+        }
+        const int64_t u0 = (int64_t)wt * WT;
+        const int slot = wt_slot(nd, u0);
+        if (slot >= 0) {
+            bool ok = true;
+            if (nd.ipop[slot].model != SZSNN_POISSON) {
+                ok = __all_sync(0xffffffffu, mbar_wait_bounded(&bar[s], (ph >> s) & 1u));
+                if (!ok) {  // report, wait once more so no copy is still writing the stage, stop
+                    if (lane == 0) dev_error(nd.err, SZSNN_DEV_WAIT_TIMEOUT, (uint32_t)u0);
+                    mbar_wait_bounded(&bar[s], (ph >> s) & 1u);
+                }
+                ph ^= 1u << s;
+                pending &= ~(1u << s);
+            }
+            wt_run_slot<FIXED>(nd, slot, inb, reg + s * SB, u0, t, ok, forced, current, out_words);
+            if (!ok) break;
+        } else {
+            const StagedPops gp{nd.pops, nd.npops};
+#pragma unroll 1
+            for (int j = 0; j < WT / 32; ++j) {
+                const int64_t id = u0 + 32 * j + lane;
+                UnitIn a;
+                load_unit(nd, inb, id, forced, current, a);
+                const bool spk = update_generic(nd, gp, id, inb, t, a);
+                __syncwarp();
+                update_spikes(nd, t, id, spk, lane, out_words);
+            }
+        }
+    }
+    if (lane == 0) {
+        for (int s = 0; s < 2; ++s)  // copies issued for a tile the loop did not reach
+            if (pending & (1u << s)) mbar_wait_bounded(&bar[s], (ph >> s) & 1u);
+        bulk_wait_read();
+    }
+    __syncwarp();
+    if (nd.overlap && gw == 0 && lane == 0) {
+        step_bookkeeping(nd, t);
+        if (((uint64_t)t ^ (uint64_t)(nd.par0 + (uint32_t)k_off)) & 1u)
+            dev_error(nd.err, SZSNN_DEV_STEP_PARITY, (uint32_t)t);
+    }
+}
+
+// update with either tile scheme (WTILES: persistent warp tiles), for update
+// block `blk` of `nblk`
+template <bool WTILES>
+__device__ __forceinline__ void update_any(const NetDev& nd, int k_off, int blk, int nblk,
+                                           const uint32_t* __restrict__ forced, const float* __restrict__ current,
+                                           uint32_t* __restrict__ out_words)
+{
+    if constexpr (WTILES) {
+        const int wpb = (int)(blockDim.x >> 5);
+        const int gw = blk * wpb + (int)(threadIdx.x >> 5), nw = nblk * wpb;
+        if (nd.acc_mode == SZSNN_ACC_FIXED) update_warp_tiles<true>(nd, k_off, gw, nw, forced, current, out_words);
+        else update_warp_tiles<false>(nd, k_off, gw, nw, forced, current, out_words);
+    } else {
+        update_body(nd, k_off, blk, forced, current, out_words);
+    }
+}
+
+// registers: block tiles keep six resident 256-thread blocks per SM (40
+// registers); warp tiles are bound by their shared-memory ring to four
+#define UPD_MIN_BLOCKS_WT 4
+
+template <bool WTILES>
+__global__ void __launch_bounds__(UPD_MAX_BLOCK, WTILES ? UPD_MIN_BLOCKS_WT : UPD_MIN_BLOCKS)
+    k_update(const __grid_constant__ NetDev nd, int k_off, const uint32_t* __restrict__ forced,
+             const float* __restrict__ current, uint32_t* __restrict__ out_words)
+{
+    update_any<WTILES>(nd, k_off, blockIdx.x, gridDim.x, forced, current, out_words);
 }
 
 // Overlapped step t in one launch: blocks 0..far_blocks-1 deliver delays >= 2
@@ -880,16 +1176,17 @@ __global__ void __launch_bounds__(UPD_MAX_BLOCK, UPD_MIN_BLOCKS) k_update(const 
 // step t (which delivers its own spikes' delay-1 buckets into step t+1).  The
 // delivery blocks come first so they are resident from the start and run
 // beside the update blocks.
-template <int G>
-__global__ void __launch_bounds__(UPD_MAX_BLOCK, UPD_MIN_BLOCKS) k_step(const __grid_constant__ NetDev nd, int k_off, int far_blocks, const uint32_t* __restrict__ forced,
-                                              const float* __restrict__ current, uint32_t* __restrict__ out_words)
+template <int G, bool WTILES>
+__global__ void __launch_bounds__(UPD_MAX_BLOCK, WTILES ? UPD_MIN_BLOCKS_WT : UPD_MIN_BLOCKS)
+    k_step(const __grid_constant__ NetDev nd, int k_off, int far_blocks, const uint32_t* __restrict__ forced,
+           const float* __restrict__ current, uint32_t* __restrict__ out_words)
 {
     if ((int)blockIdx.x < far_blocks) {  // G > 0: grouped delivery, G lanes per bucket; G < 0: flattened, -G items per warp
         if constexpr (G > 0) propagate_grouped<G>(nd, k_off + 1, 2, PF_PENDING, blockIdx.x, far_blocks);
         else propagate_flat<-G>(nd, k_off + 1, 2, PF_PENDING, blockIdx.x, far_blocks);
         return;
     }
-    update_body(nd, k_off, blockIdx.x - far_blocks, forced, current, out_words);
+    update_any<WTILES>(nd, k_off, blockIdx.x - far_blocks, gridDim.x - far_blocks, forced, current, out_words);
 }
 
 // ---- device generator (fixed fan-out), one warp per row
@@ -1045,6 +1342,7 @@ NetDev make_dev(szsnn_net* n, int par)
     d.blk_pop = n->d_blk_pop;
     d.par0 = (uint32_t)(par & 1);
     d.upt = upd_upt(n);
+    d.warp_tiles = (n->upd_tiles == 1 && n->npops <= INLINE_POPS) ? 1u : 0u;
     // parameter-table slots: the populations with shared parameters and a model
     // the inline update covers, each with the update blocks that lie inside it
     if (n->npops <= INLINE_POPS) {
@@ -1055,6 +1353,7 @@ NetDev make_dev(szsnn_net* n, int par)
                                       q.model == SZSNN_IZHIKEVICH || q.model == SZSNN_POISSON);
             const int64_t lo = sz_div_up(q.begin, bs);                        // first block starting inside
             const int64_t hi = q.end >= n->U ? sz_div_up(n->U, bs) : q.end / bs;  // blocks ending inside
+            if (ok && d.warp_tiles) { d.ipop[i] = q; continue; }  // warp tiles find their slot by unit range
             if (!ok || hi <= lo) continue;
             d.ipop[i] = q;
             d.ib_lo[i] = (int32_t)lo;
@@ -1134,6 +1433,7 @@ cudaError_t update_smem(const NetDev& d, int bs, K kernel, size_t* bytes, size_t
     bool any = false;
     for (int i = 0; i < INLINE_POPS; ++i) any = any || d.ib_hi[i] > d.ib_lo[i];
     *bytes = any ? tile_smem_bytes((int64_t)d.upt * bs, d.acc_mode == SZSNN_ACC_FIXED) : 0;
+    if (d.warp_tiles) *bytes = (size_t)(bs / 32) * wt_region_bytes(d.acc_mode == SZSNN_ACC_FIXED);
     *bytes = std::max(*bytes, floor);
     if (*bytes > 48 * 1024)
         return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*bytes);
@@ -1150,15 +1450,33 @@ cudaError_t launch_monitor(szsnn_net* n, const NetDev& d, int k_off, cudaStream_
     return cudaGetLastError();
 }
 
+// update blocks of a launch: one per tile, or the persistent warp-tile grid
+// (blocks per SM as tuned, at most one warp per warp tile)
+int64_t update_blocks(const szsnn_net* n, const NetDev& d, int bs)
+{
+    if (d.warp_tiles) {
+        const int64_t per_sm = n->upd_per_sm > 0 ? n->upd_per_sm : 2;
+        return std::max<int64_t>(1, std::min<int64_t>(sz_div_up(sz_div_up(n->U, WT), bs / 32),
+                                                      per_sm * num_sms(n->ctx)));
+    }
+    return sz_div_up(n->U, (int64_t)bs * d.upt);
+}
+
 cudaError_t launch_update(szsnn_net* n, const NetDev& d, int k_off, const uint32_t* forced, const float* cur,
                           uint32_t* words, cudaStream_t st)
 {
     int bs = n->upd_block;
-    int64_t blocks = sz_div_up(n->U, (int64_t)bs * d.upt);
+    int64_t blocks = update_blocks(n, d, bs);
     size_t smem = 0;
-    cudaError_t e = update_smem(d, bs, k_update, &smem);
+    cudaError_t e;
+    if (d.warp_tiles) {
+        e = update_smem(d, bs, k_update<true>, &smem);
+        if (e == cudaSuccess) k_update<true><<<(unsigned)blocks, bs, smem, st>>>(d, k_off, forced, cur, words);
+    } else {
+        e = update_smem(d, bs, k_update<false>, &smem);
+        if (e == cudaSuccess) k_update<false><<<(unsigned)blocks, bs, smem, st>>>(d, k_off, forced, cur, words);
+    }
     if (e != cudaSuccess) return e;
-    k_update<<<(unsigned)blocks, bs, smem, st>>>(d, k_off, forced, cur, words);
     return cudaGetLastError();
 }
 
@@ -1168,15 +1486,20 @@ cudaError_t launch_step(szsnn_net* n, const NetDev& d, int k_off, const uint32_t
 {
     const int bs = n->upd_block;
     const int far = n->D < 2 ? 0 : (n->prop_blocks > 0 ? n->prop_blocks : num_sms(n->ctx) * std::max(1, 1024 / bs));
-    const int64_t blocks = far + sz_div_up(n->U, (int64_t)bs * d.upt);
+    const int64_t blocks = far + update_blocks(n, d, bs);
     const dim3 grid((unsigned)blocks);
     size_t smem = 0;
     cudaError_t e = cudaSuccess;
     const size_t win = (far > 0 && n->prop_mode == 1) ? far_window_bytes(bs) : 0;
-#define SZ_STEP(G)                                                         \
-    do {                                                                  \
-        e = update_smem(d, bs, k_step<G>, &smem, win);                    \
-        if (e == cudaSuccess) k_step<G><<<grid, bs, smem, st>>>(d, k_off, far, forced, cur, words); \
+#define SZ_STEP(G)                                                                                       \
+    do {                                                                                                \
+        if (d.warp_tiles) {                                                                             \
+            e = update_smem(d, bs, k_step<G, true>, &smem, win);                                        \
+            if (e == cudaSuccess) k_step<G, true><<<grid, bs, smem, st>>>(d, k_off, far, forced, cur, words); \
+        } else {                                                                                        \
+            e = update_smem(d, bs, k_step<G, false>, &smem, win);                                       \
+            if (e == cudaSuccess) k_step<G, false><<<grid, bs, smem, st>>>(d, k_off, far, forced, cur, words); \
+        }                                                                                               \
     } while (0)
     if (n->prop_mode == 1) {
         switch (n->prop_group) {
@@ -1911,6 +2234,19 @@ extern "C" int szsnn_net_set_tuning(szsnn_net* n, int mode, int group, int block
     return SZSNN_OK;
 }
 
+extern "C" int szsnn_net_set_update_tiles(szsnn_net* n, int mode, int blocks_per_sm)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    if (mode != 0 && mode != 1) return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "update tile mode must be 0 or 1");
+    if (blocks_per_sm < 0 || blocks_per_sm > 32)
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "update blocks per SM must be in 0..32");
+    n->upd_tiles = mode;
+    n->upd_per_sm = blocks_per_sm;
+    for (auto& kv : n->graphs) cudaGraphExecDestroy(kv.second);
+    n->graphs.clear();
+    return SZSNN_OK;
+}
+
 extern "C" int szsnn_net_stats_get(szsnn_net* n, szsnn_net_stats* out)
 {
     if (!n || !out) return SZSNN_ERR_ARG;
@@ -2274,7 +2610,7 @@ extern "C" int szsnn_step_static(const szsnn_static_step* s, char* err, size_t e
     k_propagate<16><<<sms * 16, 256, 0, st>>>(d, 0, 1, PF_ZERO_SLOT | PF_SPIKES);
     e = cudaGetLastError();
     if (e == cudaSuccess) {
-        k_update<<<(unsigned)sz_div_up(U, 256), 256, 0, st>>>(d, 0, nullptr, nullptr, s->fired_words);
+        k_update<false><<<(unsigned)sz_div_up(U, 256), 256, 0, st>>>(d, 0, nullptr, nullptr, s->fired_words);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess)

@@ -225,6 +225,11 @@ class Network:
     def set_tuning(self, mode: int = 0, group: int = 0, blocks: int = -1, update_block: int = 0) -> None:
         L.check(self.lib.szsnn_net_set_tuning(self.h, mode, group, blocks, update_block), self.ctx.h, "set_tuning")
 
+    def set_update_tiles(self, mode: int, blocks_per_sm: int = 0) -> None:
+        """0: a block per update tile each step; 1: persistent warp tiles with
+        `blocks_per_sm` update blocks per SM (0: the default of 2)."""
+        L.check(self.lib.szsnn_net_set_update_tiles(self.h, mode, blocks_per_sm), self.ctx.h, "set_update_tiles")
+
     overlap = True
 
     def set_overlap(self, on: bool) -> None:
