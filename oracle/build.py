@@ -4,6 +4,9 @@
   oracle/_ref/libclemu_*.so    the reference's own .cl kernels under the CPU
                                work-group emulator (only where the reference
                                sources are present; see clemu/build_clemu.py)
+  oracle/_ref/refhost*         the reference's own host (Simulation, layout
+                               builders) on the szsnn C ABI through
+                               szsnn_b200/compat (see refhost/build_refhost.py)
 """
 from __future__ import annotations
 
@@ -34,6 +37,8 @@ def build_all(ref_root: str | None = None, force: bool = False) -> None:
     ref_root = ref_root or reference_root()
     if ref_root and os.path.isdir(cl_dir(ref_root)):
         build_clemu(ref_root, force)
+        from .refhost.build_refhost import build_refhost
+        build_refhost(ref_root, force)
 
 
 if __name__ == "__main__":
