@@ -394,6 +394,8 @@ def bench_batched(ctx, args):
     for k in ("looped_tuned_s", "looped_tuned_nets_per_s", "speedup_vs_tuned_loop", "loop_tuning"):
         if k in r:
             res[k] = r[k]
+    if "spikes_looped_tuned" in r:
+        res["spike_counts_equal_tuned_loop"] = bool(np.array_equal(r["spikes_batched"], r["spikes_looped_tuned"]))
     return res
 
 

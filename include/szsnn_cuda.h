@@ -285,6 +285,19 @@ int szsnn_net_destroy(szsnn_net* net);
  * optional host forced-spike words and external current, fired words out. */
 int szsnn_net_step(szsnn_net* net, const uint32_t* forced_host, const float* current_host,
                    uint32_t* fired_host);
+/* No counterpart in the reference (one device per network, Context.cpp:211-213):
+ * the exchange step of a network sharded by unit ranges across devices.
+ * words_host ([words] spike words, host memory) holds the spikes that units
+ * updated by other shards emitted in the step just done; they are appended
+ * to this network's spike ring for that step and, in the overlapped order,
+ * their delay-1 buckets delivered into the next step's inputs -- what the
+ * update does for its own spikes.  Call it after each step, before the next. */
+int szsnn_net_inject_spikes(szsnn_net* net, const uint32_t* words_host);
+/* The units this network updates when it is one shard of a network split by
+ * unit ranges: neurons [n_lo, n_hi) and sources [s_lo, s_hi); the others keep
+ * their state and never spike here (their spikes arrive by
+ * szsnn_net_inject_spikes).  Default: every unit. */
+int szsnn_net_set_owned(szsnn_net* net, int64_t n_lo, int64_t n_hi, int64_t s_lo, int64_t s_hi);
 /* `steps` steps in CUDA-graph chunks.  forced_host: [steps][words] or NULL;
  * raster_host: [steps][words] output spike words or NULL. */
 int szsnn_net_run(szsnn_net* net, int64_t steps, const uint32_t* forced_host,

@@ -118,6 +118,8 @@ SIGNATURES = {
     "szsnn_net_generate": (_I, [_P, _P, _I, _U64]),
     "szsnn_net_destroy": (_I, [_P]),
     "szsnn_net_step": (_I, [_P, _P, _P, _P]),
+    "szsnn_net_inject_spikes": (_I, [_P, _P]),
+    "szsnn_net_set_owned": (_I, [_P, _I64, _I64, _I64, _I64]),
     "szsnn_net_run": (_I, [_P, _I64, _P, _P]),
     "szsnn_net_run_device": (_I, [_P, _I64, _P, _P, _P]),
     "szsnn_net_stats_get": (_I, [_P, _P]),

@@ -58,12 +58,17 @@ def _apply(net, c: dict) -> None:
     net.set_tuning(c["mode"], c["group"], c["blocks"], c["update_block"])
 
 
-def tune(net, replays: int = 20, sms: int = 148, use_cache: bool = True) -> dict:
+def tune(net, replays: int = 20, sms: int = 148, use_cache: bool = True, cache: dict | None = None) -> dict:
     """Pick and apply the fastest step order and launch shape; returns the
-    choice and timings."""
+    choice and timings.  `cache`: a dict shared by the calls of one run in
+    place of the file cache (workloads of one size bucket tuned once)."""
     ev = net.profile_step(1)["events_per_launch"]
     key = workload_key(net, ev, sms)
-    cache = _load() if use_cache else {}
+    mem = cache is not None
+    if mem:
+        use_cache = False
+    else:
+        cache = _load() if use_cache else {}
     if key in cache:
         c = cache[key]
         _apply(net, c)
@@ -101,7 +106,8 @@ def tune(net, replays: int = 20, sms: int = 148, use_cache: bool = True) -> dict
                     best = dict(overlap=True, mode=mode, group=group, blocks=blocks, update_block=ub, step_us=us)
     choice = dict(best, classic_step_us=classic["step_us"])
     _apply(net, choice)
-    if use_cache:
+    if use_cache or mem:
         cache[key] = choice
+    if use_cache:
         _store(cache)
     return dict(choice, cached=False, key=key, trials=trials)

@@ -167,13 +167,17 @@ def single_network(ctx, spec: NetSpec, acc_mode: int = L.ACC_FLOAT, graph_chunk:
 
 def compare_batched_looped(ctx, specs: list[NetSpec], steps: int = 1000, acc_mode: int = L.ACC_FLOAT,
                            graph_chunk: int = 100, tune: bool = True, gen_seed: int = 12345,
-                           warmup: int | None = None) -> dict:
+                           warmup: int | None = None, tune_loop: bool = True) -> dict:
     """nets/s of one batched run against the plain path looped per net.
 
     Both sides are timed on the device (CUDA events on the launching stream)
     from the first step to the last, networks already built on the device;
     the looped side is the sum over nets.  Wall-clock times (with a device
-    synchronisation at each end) are reported beside them."""
+    synchronisation at each end) are reported beside them.  The loop runs
+    twice: each net in the default launch shape, and (tune_loop) each net in
+    the shape the same autotuner picks for it after the same warm-up, tuned
+    once per workload bucket (size, delays, event rate) and shared by the
+    nets of that bucket."""
     batch = Batch(ctx, specs, acc_mode, graph_chunk, gen_seed)
     warm = warmup if warmup is not None else 3 * graph_chunk
     batch.run(warm)  # graph instantiation and initial transient outside the timed region
@@ -207,12 +211,36 @@ def compare_batched_looped(ctx, specs: list[NetSpec], steps: int = 1000, acc_mod
         t_loop += net.device_ms() / 1e3
         s_loop[i] = net.group_spikes()[0]
         net.close()
-    return dict(nets=len(specs), steps=steps, batched_s=t_batch, looped_s=t_loop,
-                batched_nets_per_s=len(specs) / t_batch, looped_nets_per_s=len(specs) / t_loop,
-                speedup=t_loop / t_batch, wall_batched_s=w_batch, wall_looped_s=w_loop,
-                neurons=int(sum(s.n for s in specs)),
-                synapses=int(batch.net.n_synapses), spikes_batched=s_batch, spikes_looped=s_loop,
-                events_batched=int(st["events"]))
+    out = dict(nets=len(specs), steps=steps, batched_s=t_batch, looped_s=t_loop,
+               batched_nets_per_s=len(specs) / t_batch, looped_nets_per_s=len(specs) / t_loop,
+               speedup=t_loop / t_batch, wall_batched_s=w_batch, wall_looped_s=w_loop,
+               neurons=int(sum(s.n for s in specs)),
+               synapses=int(batch.net.n_synapses), spikes_batched=s_batch, spikes_looped=s_loop,
+               events_batched=int(st["events"]))
+    if tune_loop:
+        from .autotune import tune as _tune
+        shared: dict = {}
+        t_tuned = 0.0
+        s_tuned = np.zeros(len(specs), np.uint64)
+        for i, spec in enumerate(specs):
+            net = single_network(ctx, spec, acc_mode, graph_chunk, gen_seed)
+            net.run_device(warm)
+            ctx.sync()
+            _tune(net, replays=20, cache=shared)
+            net.run_device(graph_chunk)  # graphs of the chosen shape; the batch's warm-up length
+            ctx.sync()
+            net.group_spikes(reset=True)
+            net.run_device(steps)
+            ctx.sync()
+            t_tuned += net.device_ms() / 1e3
+            s_tuned[i] = net.group_spikes()[0]
+            net.close()
+        out.update(looped_tuned_s=t_tuned, looped_tuned_nets_per_s=len(specs) / t_tuned,
+                   speedup_vs_tuned_loop=t_tuned / t_batch, spikes_looped_tuned=s_tuned,
+                   loop_tuning={"buckets": len(shared), "shapes": sorted({(c["overlap"], c["mode"], c["group"],
+                                                                            c["blocks"], c["update_block"])
+                                                                           for c in shared.values()})})
+    return out
 
 
 def _main(argv=None) -> None:

@@ -88,7 +88,14 @@ struct NetDev {
     int32_t ib_lo[INLINE_POPS], ib_hi[INLINE_POPS];  // update blocks [lo, hi) lying inside slot i (empty: none)
     PopDev ipop[INLINE_POPS];              // populations with shared parameters, by value in the kernel parameters
     uint32_t warp_tiles;                   // 1: persistent warp-tile update (update_warp_tiles)
+    int64_t own_lo[2], own_hi[2];          // units this network updates: neurons [0], sources [1]
 };
+
+// the unit is updated here (a sharded network updates its own ranges only)
+__device__ __forceinline__ bool owned(const NetDev& nd, int64_t id)
+{
+    return (id >= nd.own_lo[0] && id < nd.own_hi[0]) || (id >= nd.own_lo[1] && id < nd.own_hi[1]);
+}
 
 struct szsnn_net {
     szsnn_ctx* ctx = nullptr;
@@ -130,6 +137,7 @@ struct szsnn_net {
     uint32_t* d_raster_stage[2] = {};
     float* d_dbg_in = nullptr;
     uint32_t* h_pinned_words = nullptr;  // pinned: one step's words (szsnn_net_step)
+    uint32_t* d_inject = nullptr;        // spike words of other shards (szsnn_net_inject_spikes)
     uint32_t* h_io[4] = {};              // pinned bounce buffers for pageable host arrays: in0, in1, out0, out1
     cudaStream_t copy_st = nullptr;      // host -> device copies of szsnn_net_run (forced words)
     cudaStream_t copy_out_st = nullptr;  // device -> host copies of szsnn_net_run (raster)
@@ -140,6 +148,7 @@ struct szsnn_net {
     uint64_t graph_launches = 0, kernel_launches = 0;
     int prop_mode = 0, prop_group = 16, prop_blocks = 0, upd_block = 256;
     int upd_tiles = 0, upd_per_sm = 0;   // update tiles: 0 block tiles, 1 persistent warp tiles (blocks per SM)
+    int64_t own_lo[2] = {0, 0}, own_hi[2] = {-1, -1};  // owned neuron / source ranges (-1: all)
     double t_prop_ms = 0, t_upd_ms = 0, t_total_ms = 0;
     cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;  // around the last szsnn_net_run*
     bool run_timed = false;
@@ -694,7 +703,7 @@ __device__ __forceinline__ void tile_run(const NetDev& nd, const InBuf& inb, int
         const uint32_t u = (uint32_t)j * bs + threadIdx.x;
         const int64_t id = tile0 + u;
         bool spk = false;
-        if (ok && id < nd.U) spk = tile_unit<MODEL, FIXED>(nd, P, inb, sm, (uint32_t)id, u, t, forced, current);
+        if (ok && id < nd.U && owned(nd, id)) spk = tile_unit<MODEL, FIXED>(nd, P, inb, sm, (uint32_t)id, u, t, forced, current);
         __syncwarp();
         update_spikes(nd, t, id, spk, lane, out_words);
     }
@@ -761,7 +770,7 @@ __device__ __forceinline__ StagedPops stage_pops(const NetDev& nd, int blk)
 __device__ __forceinline__ bool update_generic(const NetDev& nd, const StagedPops& sp_, int64_t id, const InBuf& inb,
                                                long long t, UnitIn& a)
 {
-    const bool unit = id < nd.U, neuron = id < nd.N;
+    const bool unit = id < nd.U && owned(nd, id), neuron = id < nd.N;
     const PopDev* pd = nullptr;
     if (unit) {
         if (sp_.np >= 0) {
@@ -979,7 +988,7 @@ __device__ __forceinline__ void wt_run(const NetDev& nd, const InBuf& inb, unsig
         const uint32_t u = 32u * j + lane;
         const int64_t id = u0 + u;
         bool spk = false;
-        if (ok && id < nd.U) {
+        if (ok && id < nd.U && owned(nd, id)) {
             const bool f = forced ? ((forced[id >> 5] >> (id & 31)) & 1u) != 0u : false;
             if (MODEL == SZSNN_POISSON) {
                 spk = sz_poisson_fires(P.seed, id - P.begin, t, P.p[0]) || f;
@@ -1189,6 +1198,25 @@ __global__ void __launch_bounds__(UPD_MAX_BLOCK, WTILES ? UPD_MIN_BLOCKS_WT : UP
     update_any<WTILES>(nd, k_off, blockIdx.x - far_blocks, gridDim.x - far_blocks, forced, current, out_words);
 }
 
+// Spikes of the step just done (step counter - 1) emitted by units another
+// shard updates: one warp per 32-unit word, each set bit handled as the
+// update's spike epilogue handles its own spikes (group counter, ring
+// append to slot t, and in the overlapped order the delay-1 delivery into
+// step t+1's inputs; the classic order delivers it from the ring).
+__global__ void __launch_bounds__(256) k_inject(const __grid_constant__ NetDev nd, const uint32_t* __restrict__ words)
+{
+    const long long t = *nd.clock - 1;
+    const uint32_t lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nd.words; w += nw) {
+        const uint32_t word = words[w];
+        if (!word) continue;  // warp-uniform
+        const int64_t id = w * 32 + lane;
+        const bool spk = ((word >> lane) & 1u) && id < nd.U;
+        update_spikes(nd, t, id, spk, lane, nullptr);
+    }
+}
+
 // ---- device generator (fixed fan-out), one warp per row
 struct GenDev {
     int64_t src_begin, src_count, tgt_begin, tgt_count;
@@ -1343,6 +1371,10 @@ NetDev make_dev(szsnn_net* n, int par)
     d.par0 = (uint32_t)(par & 1);
     d.upt = upd_upt(n);
     d.warp_tiles = (n->upd_tiles == 1 && n->npops <= INLINE_POPS) ? 1u : 0u;
+    d.own_lo[0] = n->own_hi[0] < 0 ? 0 : n->own_lo[0];
+    d.own_hi[0] = n->own_hi[0] < 0 ? n->N : n->own_hi[0];
+    d.own_lo[1] = n->own_hi[1] < 0 ? n->N : n->own_lo[1];
+    d.own_hi[1] = n->own_hi[1] < 0 ? n->U : n->own_hi[1];
     // parameter-table slots: the populations with shared parameters and a model
     // the inline update covers, each with the update blocks that lie inside it
     if (n->npops <= INLINE_POPS) {
@@ -1560,6 +1592,7 @@ void free_net(szsnn_net* n)
     cudaFree(n->d_stats);
     cudaFree(n->d_current_stage);
     cudaFree(n->d_dbg_in);
+    cudaFree(n->d_inject);
     if (n->h_pinned_words) cudaFreeHost(n->h_pinned_words);
     for (auto& h : n->h_io) if (h) cudaFreeHost(h);
     if (n->ev_run0) cudaEventDestroy(n->ev_run0);
@@ -1868,6 +1901,39 @@ extern "C" int szsnn_net_step(szsnn_net* n, const uint32_t* forced_host, const f
         NET_TRY(n, cudaStreamSynchronize(st));
         std::memcpy(fired_host, n->h_pinned_words, (size_t)n->words * 4);
     }
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_set_owned(szsnn_net* n, int64_t n_lo, int64_t n_hi, int64_t s_lo, int64_t s_hi)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    if (n_lo < 0 || n_lo > n_hi || n_hi > n->N || s_lo < n->N || s_lo > s_hi || s_hi > n->U)
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG,
+                               "szsnn_net_set_owned: ranges must satisfy 0 <= n_lo <= n_hi <= N <= s_lo <= s_hi <= N+P");
+    n->own_lo[0] = n_lo;
+    n->own_hi[0] = n_hi;
+    n->own_lo[1] = s_lo;
+    n->own_hi[1] = s_hi;
+    for (auto& kv : n->graphs) cudaGraphExecDestroy(kv.second);
+    n->graphs.clear();
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_inject_spikes(szsnn_net* n, const uint32_t* words_host)
+{
+    if (!n || !words_host) return n ? szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "szsnn_net_inject_spikes: null words")
+                                    : SZSNN_ERR_ARG;
+    if (n->steps_done < 1)
+        return szsnn_set_error(n->ctx, SZSNN_ERR_STATE, "szsnn_net_inject_spikes: no step has run yet");
+    cudaStream_t st = n->ctx->stream;
+    if (!n->d_inject) NET_TRY(n, dalloc(&n->d_inject, (size_t)n->words));
+    std::memcpy(n->h_pinned_words, words_host, (size_t)n->words * 4);
+    NET_TRY(n, cudaMemcpyAsync(n->d_inject, n->h_pinned_words, (size_t)n->words * 4, cudaMemcpyHostToDevice, st));
+    const int grid = (int)std::min<int64_t>(sz_div_up(n->words * 32, 256), (int64_t)num_sms(n->ctx) * 8);
+    k_inject<<<grid, 256, 0, st>>>(make_dev(n), n->d_inject);
+    NET_TRY(n, cudaGetLastError());
+    NET_TRY(n, cudaStreamSynchronize(st));  // the pinned staging buffer is free again on return
+    n->kernel_launches += 1;
     return SZSNN_OK;
 }
 

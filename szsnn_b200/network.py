@@ -154,6 +154,18 @@ class Network:
                                         None if out is None else out.ctypes.data), self.ctx.h, "net_step")
         return out
 
+    def set_owned(self, n_lo: int, n_hi: int, s_lo: int, s_hi: int) -> None:
+        """Update only neurons [n_lo, n_hi) and sources [s_lo, s_hi) (one shard)."""
+        L.check(self.lib.szsnn_net_set_owned(self.h, n_lo, n_hi, s_lo, s_hi), self.ctx.h, "set_owned")
+
+    def inject_spikes(self, words) -> None:
+        """Spike words of the step just done from units other shards update
+        (szsnn_net_inject_spikes)."""
+        w = np.ascontiguousarray(words, np.uint32)
+        if w.shape != (self.words,):
+            raise ValueError("inject_spikes takes one step's words")
+        L.check(self.lib.szsnn_net_inject_spikes(self.h, w.ctypes.data), self.ctx.h, "inject_spikes")
+
     def run(self, steps: int, forced_words=None, raster=True, out=None) -> np.ndarray | None:
         """`steps` steps from the host: forced-spike words [steps, words] in,
         raster words [steps, words] out.  Page-locked arrays (`out`, or

@@ -108,6 +108,38 @@ def test_gradients_match_fp64_bptt(ck, N, B, shuffle):
             assert np.max(np.abs(ref)) > 0
 
 
+def test_full_size_gradients_match_fp64_bptt():
+    """The benchmark's shape (N = 10,000, 10 % recurrent, M = 700 inputs,
+    K = 20 readouts, B = 64 trials) over a short horizon: gradients within
+    1e-4 of FP64 BPTT on the GPU's own trajectory."""
+    net, w_in, val, w_out, x, v0 = _setup(N=10000, M=700, K=20, B=64, T=20, w_in_scale=1.0)
+    for t in (w_in, val, w_out):
+        t.requires_grad_(True)
+    ymax, vsum = P.LIFCurrExpFunction.apply(w_in, val, w_out, x, v0, net)
+    g = torch.Generator(device="cpu").manual_seed(2)
+    gy = torch.randn(ymax.shape, generator=g).cuda()
+    gv = (torch.randn(vsum.shape, generator=g) * 1e-3).cuda()
+    (ymax * gy).sum().add_((vsum * gv).sum()).backward()
+    torch.cuda.synchronize()
+    out = P.simulate(net, w_in.detach(), val.detach(), w_out.detach(), x, v0, trace_u=True)
+    S = P.unpack_bits(out["spikes"], net.n_neurons).cpu().numpy()
+    assert S.sum() > 1000
+    xs = P.unpack_bits(x, net.n_inputs).cpu().numpy()
+    p = dict(net.params, alpha=net.alpha)
+    Wd = _dense(net, val)
+    fw = R.forward(p, w_in.detach().cpu().numpy(), Wd, w_out.detach().cpu().numpy(), xs, v0.cpu().numpy(), spikes=S)
+    fw_gpu = dict(fw, U=out["u_trace"].cpu().numpy().astype(np.float64))
+    dWin, dWrec, dWout = R.backward(p, w_in.detach().cpu().numpy(), Wd, w_out.detach().cpu().numpy(), xs, fw_gpu,
+                                    gy.cpu().numpy(), gv.cpu().numpy(), beta=net.beta)
+    rp, col = net.rec_row_ptr.cpu().numpy(), net.rec_col.cpu().numpy()
+    rows = np.repeat(np.arange(net.n_neurons), np.diff(rp))
+    for got, ref in ((w_in.grad, dWin), (val.grad, dWrec[rows, col]), (w_out.grad, dWout)):
+        got = got.cpu().numpy().astype(np.float64)
+        err = np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-30)
+        assert err <= 1e-4, err
+        assert np.max(np.abs(ref)) > 0
+
+
 def test_finite_differences_subthreshold():
     """Below threshold the layer is linear in w_in on each sign pattern of the
     weights (the sign picks the exc / inh synaptic channel), so a central
