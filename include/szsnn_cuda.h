@@ -359,9 +359,11 @@ int szsnn_net_set_tuning(szsnn_net* net, int propagate_mode, int group, int prop
 /* Update tiles: mode 0 = one tile per update block, a new block per tile each
  * step; mode 1 = persistent warp tiles: blocks_per_sm update blocks per SM
  * (0 = 2), each warp streaming 128-unit tiles through a two-stage ring of
- * bulk copies in shared memory and writing them back with bulk stores.  Mode
- * 1 applies to networks of at most four populations; others keep mode 0.
- * Results are identical in both modes. */
+ * bulk copies in shared memory and writing them back with bulk stores (for
+ * networks of at most four populations; others keep mode 0); mode 2 =
+ * persistent block tiles: the tiles of mode 0 taken in turn by as many update
+ * blocks as stay resident (blocks_per_sm, or 0 = from the occupancy of the
+ * launch).  Results are identical in every mode. */
 int szsnn_net_set_update_tiles(szsnn_net* net, int mode, int blocks_per_sm);
 /* Step order.  1 (default): overlapped -- input buffers double-buffered by
  * step parity, delivery of delays >= 2 into step t+1 runs in the same launch

@@ -87,7 +87,8 @@ struct NetDev {
     int32_t upt;                           // units per update thread (1..UPD_UPT)
     int32_t ib_lo[INLINE_POPS], ib_hi[INLINE_POPS];  // update blocks [lo, hi) lying inside slot i (empty: none)
     PopDev ipop[INLINE_POPS];              // populations with shared parameters, by value in the kernel parameters
-    uint32_t warp_tiles;                   // 1: persistent warp-tile update (update_warp_tiles)
+    uint32_t tiles;                        // update tile scheme: 0 a block per tile, 1 persistent warp tiles,
+                                           // 2 persistent block tiles
     int64_t own_lo[2], own_hi[2];          // units this network updates: neurons [0], sources [1]
 };
 
@@ -609,24 +610,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
     return ok != 0u;
 }
 
-// bounded wait for phase 0 of the tile's mbarrier
-__device__ __forceinline__ bool tile_wait(uint64_t* bar)
+// bounded wait for the phase of the tile's mbarrier with parity `parity`
+__device__ __forceinline__ bool tile_wait(uint64_t* bar, uint32_t parity = 0u)
 {
     for (int i = 0; i < (1 << 20); ++i)
-        if (mbar_try_wait(bar, 0u)) return true;
+        if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
 
 // Issue the tile's bulk copies (thread 0) and wait for them (all threads).
 // Model M decides which arrays a unit reads; Poisson tiles read none.
+// phase < 0: a block with one tile (the mbarrier is initialised here and its
+// phase 0 awaited); phase >= 0: a persistent block whose mbarrier was
+// initialised once, awaiting the phase of this tile's parity.
 template <int MODEL, bool FIXED>
 __device__ __forceinline__ bool tile_load(const NetDev& nd, const InBuf& inb, int64_t tile0, uint32_t T,
-                                          const TileSmem& sm)
+                                          const TileSmem& sm, int phase = -1)
 {
     if (MODEL == SZSNN_POISSON) return true;
     if (threadIdx.x == 0) {  // init, then the copies at once; the block barrier below orders the waits after the init
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(sm.bar)) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (phase < 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(sm.bar)) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
         const int64_t n = min((int64_t)T, nd.U - tile0);  // the tile lies inside a neuron population
         const uint32_t b4 = (uint32_t)((n * 4 + 15) & ~(int64_t)15);
         const uint32_t b8 = (uint32_t)((n * 8 + 15) & ~(int64_t)15);
@@ -645,11 +651,12 @@ __device__ __forceinline__ bool tile_load(const NetDev& nd, const InBuf& inb, in
         }
     }
     __syncthreads();
-    if (tile_wait(sm.bar)) return true;
+    const uint32_t parity = phase < 0 ? 0u : (uint32_t)(phase & 1);
+    if (tile_wait(sm.bar, parity)) return true;
     // the copies did not complete in time: report, wait once more so none is
     // still writing shared memory when the block leaves, skip the tile
     if (threadIdx.x == 0) dev_error(nd.err, SZSNN_DEV_WAIT_TIMEOUT, (uint32_t)tile0);
-    tile_wait(sm.bar);
+    tile_wait(sm.bar, parity);
     return false;
 }
 
@@ -692,11 +699,11 @@ __device__ __forceinline__ bool tile_unit(const NetDev& nd, const PopDev& P, con
 template <int MODEL, bool FIXED, int PI>
 __device__ __forceinline__ void tile_run(const NetDev& nd, const InBuf& inb, int64_t tile0, long long t,
                                         const uint32_t* __restrict__ forced, const float* __restrict__ current,
-                                        uint32_t* __restrict__ out_words, unsigned char* smem)
+                                        uint32_t* __restrict__ out_words, unsigned char* smem, int phase)
 {
     const uint32_t bs = blockDim.x, T = (uint32_t)nd.upt * bs, lane = threadIdx.x & 31;
     const TileSmem sm = tile_smem(smem, T, FIXED);
-    const bool ok = tile_load<MODEL, FIXED>(nd, inb, tile0, T, sm);
+    const bool ok = tile_load<MODEL, FIXED>(nd, inb, tile0, T, sm, phase);
     const PopDev& P = nd.ipop[PI];
 #pragma unroll 1
     for (int j = 0; j < nd.upt; ++j) {
@@ -712,27 +719,27 @@ __device__ __forceinline__ void tile_run(const NetDev& nd, const InBuf& inb, int
 template <bool FIXED, int PI>
 __device__ __forceinline__ void tile_run_pop(const NetDev& nd, const InBuf& inb, int64_t tile0, long long t,
                                             const uint32_t* __restrict__ forced, const float* __restrict__ current,
-                                            uint32_t* __restrict__ out_words, unsigned char* smem)
+                                            uint32_t* __restrict__ out_words, unsigned char* smem, int phase)
 {
     switch (nd.ipop[PI].model) {
-    case SZSNN_IF_CURR_EXP: tile_run<SZSNN_IF_CURR_EXP, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem); break;
-    case SZSNN_IF_COND_EXP: tile_run<SZSNN_IF_COND_EXP, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem); break;
-    case SZSNN_IZHIKEVICH: tile_run<SZSNN_IZHIKEVICH, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem); break;
-    default: tile_run<SZSNN_POISSON, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem); break;
+    case SZSNN_IF_CURR_EXP: tile_run<SZSNN_IF_CURR_EXP, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem, phase); break;
+    case SZSNN_IF_COND_EXP: tile_run<SZSNN_IF_COND_EXP, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem, phase); break;
+    case SZSNN_IZHIKEVICH: tile_run<SZSNN_IZHIKEVICH, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem, phase); break;
+    default: tile_run<SZSNN_POISSON, FIXED, PI>(nd, inb, tile0, t, forced, current, out_words, smem, phase); break;
     }
 }
 
 template <bool FIXED>
 __device__ __forceinline__ void tile_run_slot(const NetDev& nd, int slot, const InBuf& inb, int64_t tile0, long long t,
                                              const uint32_t* __restrict__ forced, const float* __restrict__ current,
-                                             uint32_t* __restrict__ out_words, unsigned char* smem)
+                                             uint32_t* __restrict__ out_words, unsigned char* smem, int phase)
 {
     static_assert(INLINE_POPS == 4, "one case per parameter-table slot");
     switch (slot) {
-    case 0: tile_run_pop<FIXED, 0>(nd, inb, tile0, t, forced, current, out_words, smem); break;
-    case 1: tile_run_pop<FIXED, 1>(nd, inb, tile0, t, forced, current, out_words, smem); break;
-    case 2: tile_run_pop<FIXED, 2>(nd, inb, tile0, t, forced, current, out_words, smem); break;
-    default: tile_run_pop<FIXED, 3>(nd, inb, tile0, t, forced, current, out_words, smem); break;
+    case 0: tile_run_pop<FIXED, 0>(nd, inb, tile0, t, forced, current, out_words, smem, phase); break;
+    case 1: tile_run_pop<FIXED, 1>(nd, inb, tile0, t, forced, current, out_words, smem, phase); break;
+    case 2: tile_run_pop<FIXED, 2>(nd, inb, tile0, t, forced, current, out_words, smem, phase); break;
+    default: tile_run_pop<FIXED, 3>(nd, inb, tile0, t, forced, current, out_words, smem, phase); break;
     }
 }
 
@@ -843,8 +850,11 @@ __device__ __forceinline__ void load_unit(const NetDev& nd, const InBuf& inb, in
 // sub-tile are 32 consecutive ids (one raster word).
 // Overlapped stepping: the warps with spikes deliver their units' m = 1
 // buckets into the buffer of t+1, and block 0 does the per-step bookkeeping.
-__device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk, const uint32_t* __restrict__ forced,
-                                            const float* __restrict__ current, uint32_t* __restrict__ out_words)
+// phase: -1 for a block with one tile, else the persistent block's count of
+// loaded tiles so far.  Returns whether this tile used the mbarrier.
+__device__ __forceinline__ bool update_body(const NetDev& nd, int k_off, int blk, const uint32_t* __restrict__ forced,
+                                            const float* __restrict__ current, uint32_t* __restrict__ out_words,
+                                            int phase = -1)
 {
     extern __shared__ __align__(128) unsigned char upd_smem[];
     const uint32_t bs = blockDim.x;
@@ -856,9 +866,11 @@ __device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk
 #pragma unroll
     for (int i = 0; i < INLINE_POPS; ++i)
         if (blk >= nd.ib_lo[i] && blk < nd.ib_hi[i]) slot = i;
+    bool used = false;
     if (slot >= 0) {
-        if (nd.acc_mode == SZSNN_ACC_FIXED) tile_run_slot<true>(nd, slot, inb, tile0, t, forced, current, out_words, upd_smem);
-        else tile_run_slot<false>(nd, slot, inb, tile0, t, forced, current, out_words, upd_smem);
+        if (nd.acc_mode == SZSNN_ACC_FIXED) tile_run_slot<true>(nd, slot, inb, tile0, t, forced, current, out_words, upd_smem, phase);
+        else tile_run_slot<false>(nd, slot, inb, tile0, t, forced, current, out_words, upd_smem, phase);
+        used = nd.ipop[slot].model != SZSNN_POISSON;
     } else {
         const StagedPops sp_ = stage_pops(nd, blk);
 #pragma unroll 1
@@ -878,6 +890,7 @@ __device__ __forceinline__ void update_body(const NetDev& nd, int k_off, int blk
         if (((uint64_t)t ^ (uint64_t)(nd.par0 + (uint32_t)k_off)) & 1u)
             dev_error(nd.err, SZSNN_DEV_STEP_PARITY, (uint32_t)t);
     }
+    return used;
 }
 
 // ---- persistent warp tiles
@@ -1151,18 +1164,49 @@ __device__ __forceinline__ void update_warp_tiles(const NetDev& nd, int k_off, i
     }
 }
 
-// update with either tile scheme (WTILES: persistent warp tiles), for update
-// block `blk` of `nblk`
-template <bool WTILES>
+// Persistent block tiles: update block blk of nblk takes tiles blk, blk +
+// nblk, ... of the block-tile scheme, one after the other, with one
+// mbarrier (initialised once) whose phase per loaded tile the block counts;
+// a block barrier separates the tiles (shared memory reused).  Blocks are
+// launched once per step, as many as stay resident, so no block is
+// scheduled mid-step and no partial wave trails the launch.
+__device__ __forceinline__ void update_persistent(const NetDev& nd, int k_off, int blk, int nblk,
+                                                  const uint32_t* __restrict__ forced,
+                                                  const float* __restrict__ current, uint32_t* __restrict__ out_words)
+{
+    extern __shared__ __align__(128) unsigned char upd_smem[];
+    const int64_t ntiles = sz_div_up(nd.U, (int64_t)nd.upt * blockDim.x);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(upd_smem)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __shared__ int s_stop;
+    __syncthreads();
+    int phase = 0;
+    for (int64_t tile = blk; tile < ntiles; tile += nblk) {
+        if (update_body(nd, k_off, (int)tile, forced, current, out_words, phase)) ++phase;
+        // a bulk-copy wait that ran out (device error 7) ends the block's
+        // tiles: a copy might still be in flight into its shared memory
+        if (threadIdx.x == 0) s_stop = *reinterpret_cast<volatile uint32_t*>(nd.err) == SZSNN_DEV_WAIT_TIMEOUT;
+        __syncthreads();  // every thread is done with the tile's shared memory
+        if (s_stop) break;
+    }
+}
+
+// update with one tile scheme (MODE 0: a block per tile, 1: persistent warp
+// tiles, 2: persistent block tiles), for update block `blk` of `nblk`
+template <int MODE>
 __device__ __forceinline__ void update_any(const NetDev& nd, int k_off, int blk, int nblk,
                                            const uint32_t* __restrict__ forced, const float* __restrict__ current,
                                            uint32_t* __restrict__ out_words)
 {
-    if constexpr (WTILES) {
+    if constexpr (MODE == 1) {
         const int wpb = (int)(blockDim.x >> 5);
         const int gw = blk * wpb + (int)(threadIdx.x >> 5), nw = nblk * wpb;
         if (nd.acc_mode == SZSNN_ACC_FIXED) update_warp_tiles<true>(nd, k_off, gw, nw, forced, current, out_words);
         else update_warp_tiles<false>(nd, k_off, gw, nw, forced, current, out_words);
+    } else if constexpr (MODE == 2) {
+        update_persistent(nd, k_off, blk, nblk, forced, current, out_words);
     } else {
         update_body(nd, k_off, blk, forced, current, out_words);
     }
@@ -1172,12 +1216,12 @@ __device__ __forceinline__ void update_any(const NetDev& nd, int k_off, int blk,
 // registers); warp tiles are bound by their shared-memory ring to four
 #define UPD_MIN_BLOCKS_WT 4
 
-template <bool WTILES>
-__global__ void __launch_bounds__(UPD_MAX_BLOCK, WTILES ? UPD_MIN_BLOCKS_WT : UPD_MIN_BLOCKS)
+template <int MODE>
+__global__ void __launch_bounds__(UPD_MAX_BLOCK, MODE == 1 ? UPD_MIN_BLOCKS_WT : UPD_MIN_BLOCKS)
     k_update(const __grid_constant__ NetDev nd, int k_off, const uint32_t* __restrict__ forced,
              const float* __restrict__ current, uint32_t* __restrict__ out_words)
 {
-    update_any<WTILES>(nd, k_off, blockIdx.x, gridDim.x, forced, current, out_words);
+    update_any<MODE>(nd, k_off, blockIdx.x, gridDim.x, forced, current, out_words);
 }
 
 // Overlapped step t in one launch: blocks 0..far_blocks-1 deliver delays >= 2
@@ -1185,8 +1229,8 @@ __global__ void __launch_bounds__(UPD_MAX_BLOCK, WTILES ? UPD_MIN_BLOCKS_WT : UP
 // step t (which delivers its own spikes' delay-1 buckets into step t+1).  The
 // delivery blocks come first so they are resident from the start and run
 // beside the update blocks.
-template <int G, bool WTILES>
-__global__ void __launch_bounds__(UPD_MAX_BLOCK, WTILES ? UPD_MIN_BLOCKS_WT : UPD_MIN_BLOCKS)
+template <int G, int MODE>
+__global__ void __launch_bounds__(UPD_MAX_BLOCK, MODE == 1 ? UPD_MIN_BLOCKS_WT : UPD_MIN_BLOCKS)
     k_step(const __grid_constant__ NetDev nd, int k_off, int far_blocks, const uint32_t* __restrict__ forced,
            const float* __restrict__ current, uint32_t* __restrict__ out_words)
 {
@@ -1195,7 +1239,7 @@ __global__ void __launch_bounds__(UPD_MAX_BLOCK, WTILES ? UPD_MIN_BLOCKS_WT : UP
         else propagate_flat<-G>(nd, k_off + 1, 2, PF_PENDING, blockIdx.x, far_blocks);
         return;
     }
-    update_any<WTILES>(nd, k_off, blockIdx.x - far_blocks, gridDim.x - far_blocks, forced, current, out_words);
+    update_any<MODE>(nd, k_off, blockIdx.x - far_blocks, gridDim.x - far_blocks, forced, current, out_words);
 }
 
 // Spikes of the step just done (step counter - 1) emitted by units another
@@ -1370,7 +1414,7 @@ NetDev make_dev(szsnn_net* n, int par)
     d.blk_pop = n->d_blk_pop;
     d.par0 = (uint32_t)(par & 1);
     d.upt = upd_upt(n);
-    d.warp_tiles = (n->upd_tiles == 1 && n->npops <= INLINE_POPS) ? 1u : 0u;
+    d.tiles = n->upd_tiles == 2 ? 2u : (n->upd_tiles == 1 && n->npops <= INLINE_POPS) ? 1u : 0u;
     d.own_lo[0] = n->own_hi[0] < 0 ? 0 : n->own_lo[0];
     d.own_hi[0] = n->own_hi[0] < 0 ? n->N : n->own_hi[0];
     d.own_lo[1] = n->own_hi[1] < 0 ? n->N : n->own_lo[1];
@@ -1385,7 +1429,7 @@ NetDev make_dev(szsnn_net* n, int par)
                                       q.model == SZSNN_IZHIKEVICH || q.model == SZSNN_POISSON);
             const int64_t lo = sz_div_up(q.begin, bs);                        // first block starting inside
             const int64_t hi = q.end >= n->U ? sz_div_up(n->U, bs) : q.end / bs;  // blocks ending inside
-            if (ok && d.warp_tiles) { d.ipop[i] = q; continue; }  // warp tiles find their slot by unit range
+            if (ok && d.tiles == 1) { d.ipop[i] = q; continue; }  // warp tiles find their slot by unit range
             if (!ok || hi <= lo) continue;
             d.ipop[i] = q;
             d.ib_lo[i] = (int32_t)lo;
@@ -1465,7 +1509,7 @@ cudaError_t update_smem(const NetDev& d, int bs, K kernel, size_t* bytes, size_t
     bool any = false;
     for (int i = 0; i < INLINE_POPS; ++i) any = any || d.ib_hi[i] > d.ib_lo[i];
     *bytes = any ? tile_smem_bytes((int64_t)d.upt * bs, d.acc_mode == SZSNN_ACC_FIXED) : 0;
-    if (d.warp_tiles) *bytes = (size_t)(bs / 32) * wt_region_bytes(d.acc_mode == SZSNN_ACC_FIXED);
+    if (d.tiles == 1) *bytes = (size_t)(bs / 32) * wt_region_bytes(d.acc_mode == SZSNN_ACC_FIXED);
     *bytes = std::max(*bytes, floor);
     if (*bytes > 48 * 1024)
         return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*bytes);
@@ -1486,7 +1530,7 @@ cudaError_t launch_monitor(szsnn_net* n, const NetDev& d, int k_off, cudaStream_
 // (blocks per SM as tuned, at most one warp per warp tile)
 int64_t update_blocks(const szsnn_net* n, const NetDev& d, int bs)
 {
-    if (d.warp_tiles) {
+    if (d.tiles == 1) {
         const int64_t per_sm = n->upd_per_sm > 0 ? n->upd_per_sm : 2;
         return std::max<int64_t>(1, std::min<int64_t>(sz_div_up(sz_div_up(n->U, WT), bs / 32),
                                                       per_sm * num_sms(n->ctx)));
@@ -1494,23 +1538,47 @@ int64_t update_blocks(const szsnn_net* n, const NetDev& d, int bs)
     return sz_div_up(n->U, (int64_t)bs * d.upt);
 }
 
+// persistent block tiles: as many update blocks as stay resident beside the
+// `far` delivery blocks (or the tuned count per SM), at most one per tile
+template <class K>
+int64_t persistent_blocks(const szsnn_net* n, const NetDev& d, K kernel, int bs, size_t smem, int64_t far)
+{
+    const int64_t sms = num_sms(n->ctx), tiles = sz_div_up(n->U, (int64_t)bs * d.upt);
+    int64_t total;
+    if (n->upd_per_sm > 0) {
+        total = (int64_t)n->upd_per_sm * sms;
+    } else {
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, bs, smem) != cudaSuccess || occ < 1) {
+            cudaGetLastError();
+            occ = 1;
+        }
+        total = std::max<int64_t>(sms, occ * sms - far);
+    }
+    return std::max<int64_t>(1, std::min<int64_t>(total, tiles));
+}
+
+template <int MODE>
+cudaError_t launch_update_mode(szsnn_net* n, const NetDev& d, int k_off, const uint32_t* forced, const float* cur,
+                               uint32_t* words, cudaStream_t st)
+{
+    const int bs = n->upd_block;
+    size_t smem = 0;
+    cudaError_t e = update_smem(d, bs, k_update<MODE>, &smem);
+    if (e != cudaSuccess) return e;
+    const int64_t blocks = MODE == 2 ? persistent_blocks(n, d, k_update<MODE>, bs, smem, 0) : update_blocks(n, d, bs);
+    k_update<MODE><<<(unsigned)blocks, bs, smem, st>>>(d, k_off, forced, cur, words);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_update(szsnn_net* n, const NetDev& d, int k_off, const uint32_t* forced, const float* cur,
                           uint32_t* words, cudaStream_t st)
 {
-    int bs = n->upd_block;
-    int64_t blocks = update_blocks(n, d, bs);
-    size_t smem = 0;
-    cudaError_t e;
-    if (d.warp_tiles) {
-        e = update_smem(d, bs, k_update<true>, &smem);
-        if (e == cudaSuccess) k_update<true><<<(unsigned)blocks, bs, smem, st>>>(d, k_off, forced, cur, words);
-    } else {
-        e = update_smem(d, bs, k_update<false>, &smem);
-        if (e == cudaSuccess) k_update<false><<<(unsigned)blocks, bs, smem, st>>>(d, k_off, forced, cur, words);
-    }
-    if (e != cudaSuccess) return e;
-    return cudaGetLastError();
+    if (d.tiles == 1) return launch_update_mode<1>(n, d, k_off, forced, cur, words, st);
+    if (d.tiles == 2) return launch_update_mode<2>(n, d, k_off, forced, cur, words, st);
+    return launch_update_mode<0>(n, d, k_off, forced, cur, words, st);
 }
+
 
 // overlapped step clock + k_off: far delivery into step t+1 and update(t) in one launch
 cudaError_t launch_step(szsnn_net* n, const NetDev& d, int k_off, const uint32_t* forced, const float* cur,
@@ -1518,20 +1586,21 @@ cudaError_t launch_step(szsnn_net* n, const NetDev& d, int k_off, const uint32_t
 {
     const int bs = n->upd_block;
     const int far = n->D < 2 ? 0 : (n->prop_blocks > 0 ? n->prop_blocks : num_sms(n->ctx) * std::max(1, 1024 / bs));
-    const int64_t blocks = far + update_blocks(n, d, bs);
-    const dim3 grid((unsigned)blocks);
+    const size_t win = (far > 0 && n->prop_mode == 1) ? far_window_bytes(bs) : 0;
     size_t smem = 0;
     cudaError_t e = cudaSuccess;
-    const size_t win = (far > 0 && n->prop_mode == 1) ? far_window_bytes(bs) : 0;
-#define SZ_STEP(G)                                                                                       \
-    do {                                                                                                \
-        if (d.warp_tiles) {                                                                             \
-            e = update_smem(d, bs, k_step<G, true>, &smem, win);                                        \
-            if (e == cudaSuccess) k_step<G, true><<<grid, bs, smem, st>>>(d, k_off, far, forced, cur, words); \
-        } else {                                                                                        \
-            e = update_smem(d, bs, k_step<G, false>, &smem, win);                                       \
-            if (e == cudaSuccess) k_step<G, false><<<grid, bs, smem, st>>>(d, k_off, far, forced, cur, words); \
-        }                                                                                               \
+#define SZ_STEP_MODE(G, M)                                                                                     \
+    do {                                                                                                      \
+        e = update_smem(d, bs, k_step<G, M>, &smem, win);                                                     \
+        if (e != cudaSuccess) break;                                                                          \
+        const int64_t ub = M == 2 ? persistent_blocks(n, d, k_step<G, M>, bs, smem, far) : update_blocks(n, d, bs); \
+        k_step<G, M><<<(unsigned)(far + ub), bs, smem, st>>>(d, k_off, far, forced, cur, words);             \
+    } while (0)
+#define SZ_STEP(G)                                        \
+    do {                                                  \
+        if (d.tiles == 1) SZ_STEP_MODE(G, 1);             \
+        else if (d.tiles == 2) SZ_STEP_MODE(G, 2);        \
+        else SZ_STEP_MODE(G, 0);                          \
     } while (0)
     if (n->prop_mode == 1) {
         switch (n->prop_group) {
@@ -1548,6 +1617,7 @@ cudaError_t launch_step(szsnn_net* n, const NetDev& d, int k_off, const uint32_t
         }
     }
 #undef SZ_STEP
+#undef SZ_STEP_MODE
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -2303,7 +2373,7 @@ extern "C" int szsnn_net_set_tuning(szsnn_net* n, int mode, int group, int block
 extern "C" int szsnn_net_set_update_tiles(szsnn_net* n, int mode, int blocks_per_sm)
 {
     if (!n) return SZSNN_ERR_ARG;
-    if (mode != 0 && mode != 1) return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "update tile mode must be 0 or 1");
+    if (mode < 0 || mode > 2) return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "update tile mode must be 0, 1 or 2");
     if (blocks_per_sm < 0 || blocks_per_sm > 32)
         return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "update blocks per SM must be in 0..32");
     n->upd_tiles = mode;
@@ -2676,7 +2746,7 @@ extern "C" int szsnn_step_static(const szsnn_static_step* s, char* err, size_t e
     k_propagate<16><<<sms * 16, 256, 0, st>>>(d, 0, 1, PF_ZERO_SLOT | PF_SPIKES);
     e = cudaGetLastError();
     if (e == cudaSuccess) {
-        k_update<false><<<(unsigned)sz_div_up(U, 256), 256, 0, st>>>(d, 0, nullptr, nullptr, s->fired_words);
+        k_update<0><<<(unsigned)sz_div_up(U, 256), 256, 0, st>>>(d, 0, nullptr, nullptr, s->fired_words);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess)

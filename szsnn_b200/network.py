@@ -239,7 +239,8 @@ class Network:
 
     def set_update_tiles(self, mode: int, blocks_per_sm: int = 0) -> None:
         """0: a block per update tile each step; 1: persistent warp tiles with
-        `blocks_per_sm` update blocks per SM (0: the default of 2)."""
+        `blocks_per_sm` update blocks per SM (0: the default of 2); 2:
+        persistent block tiles (`blocks_per_sm`, 0: as many as stay resident)."""
         L.check(self.lib.szsnn_net_set_update_tiles(self.h, mode, blocks_per_sm), self.ctx.h, "set_update_tiles")
 
     overlap = True

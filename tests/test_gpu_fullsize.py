@@ -65,10 +65,10 @@ def _oracle_net(csr, dtype=np.float32):
     return oracle.OracleNet(n, p, D, pops, csr, state=init_state(n, p, SEED), dtype=dtype)
 
 
-@pytest.mark.parametrize("tiles", [0, 1], ids=["block_tiles", "warp_tiles"])
+@pytest.mark.parametrize("tiles", [0, 1, 2], ids=["block_tiles", "warp_tiles", "persistent_block_tiles"])
 def test_full_size_fixed_point_equals_oracle(ctx, full_csr, tiles):
     net = _bench_net(ctx, True)
-    net.set_update_tiles(tiles, 2)
+    net.set_update_tiles(tiles, 2 if tiles == 1 else 0)
     r_gpu = net.run(100)
     on = _oracle_net(full_csr)
     r_orc, ev = on.run(100, acc_mode=oracle.ACC_FIXED, nthreads=THREADS)

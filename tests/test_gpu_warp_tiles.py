@@ -1,5 +1,6 @@
-"""GPU: the persistent warp-tile update (szsnn_net_set_update_tiles mode 1)
-against the oracle, bit for bit in fixed-point accumulation.
+"""GPU: the persistent update tile schemes (szsnn_net_set_update_tiles mode 1,
+warp tiles, and mode 2, persistent block tiles) against the oracle, bit for
+bit in fixed-point accumulation.
 
 Each warp of the update grid streams 128-unit tiles through a two-stage
 shared-memory ring (bulk copies in, bulk stores out); tiles that straddle a
@@ -11,8 +12,10 @@ population boundary run the generic per-unit update.  Covered:
   * a network whose unit count is not a multiple of 128 (the last tile is
     short and its bulk transfers are rounded to 16 bytes);
   * populations whose boundaries fall inside warp tiles (generic tiles);
-  * switching between block tiles and warp tiles mid-run;
+  * switching between the three schemes mid-run;
   * fp32 accumulation with dyadic weights (exact sums in any order).
+Persistent block tiles take the block tiles of mode 0 in turn, one mbarrier
+phase per loaded tile, in blocks that stay resident for the whole launch.
 """
 import numpy as np
 import pytest
@@ -38,14 +41,15 @@ def _spikes(r):
     return int(np.unpackbits(r.view(np.uint8)).sum())
 
 
-@pytest.mark.parametrize("overlap,per_sm", [(True, 1), (True, 3), (False, 2)])
-def test_warp_tiles_cond_equal_oracle(ctx, overlap, per_sm):
+@pytest.mark.parametrize("mode,overlap,per_sm", [(1, True, 1), (1, True, 3), (1, False, 2), (2, True, 0),
+                                                 (2, False, 0), (2, True, 1)])
+def test_warp_tiles_cond_equal_oracle(ctx, mode, overlap, per_sm):
     n, p, D = 100_000, 10_000, 16
     blocks, pops, st = cond_network(n, p, fanout=40, D=D, seed=8)
     net = sz.Network(ctx, n, p, D, pops, state=st, acc_mode=L.ACC_FIXED, graph_chunk=25)
     net.generate(blocks, seed=77)
     net.set_overlap(overlap)
-    net.set_update_tiles(1, per_sm)
+    net.set_update_tiles(mode, per_sm)
     on = oracle.OracleNet(n, p, D, pops, oracle.generate(blocks, 77, n + p, D), state=st)
     r = net.run(60)
     ro, ev = on.run(60, acc_mode=oracle.ACC_FIXED)
@@ -58,14 +62,15 @@ def test_warp_tiles_cond_equal_oracle(ctx, overlap, per_sm):
     net.close()
 
 
-def test_warp_tiles_forced_if_curr_exp(ctx):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_warp_tiles_forced_if_curr_exp(ctx, mode):
     n = 110_000
     net_ = if_network(n=n, n_syn=40 * n, max_delay=8, dyadic=False, seed=12)
     csr = sz.csr_from_synapses(n, 8, net_["src"], net_["tgt"], net_["w"], net_["d1"])
     pops = [sz.Pop(sz.IF_CURR_EXP, 0, n, net_["pv"])]
     st = [net_["v0"], None, None, np.full(n, 1e4, np.float32)]
     net = sz.Network(ctx, n, 0, 8, pops, csr=csr, state=st, acc_mode=L.ACC_FIXED, graph_chunk=25)
-    net.set_update_tiles(1, 2)
+    net.set_update_tiles(mode, 2 if mode == 1 else 0)
     on = oracle.OracleNet(n, 0, 8, pops, csr, state=st)
     fw = forced_words(forced_schedule(n, 40), n)
     r = net.run(40, forced_words=fw)
@@ -78,7 +83,8 @@ def test_warp_tiles_forced_if_curr_exp(ctx):
     net.close()
 
 
-def test_warp_tiles_izhikevich_current_short_last_tile(ctx):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_warp_tiles_izhikevich_current_short_last_tile(ctx, mode):
     """Izhikevich in 2 x 0.5 ms half-steps with a thalamic current; 50,003
     units, so the last warp tile holds 83 units."""
     n = 50_003
@@ -91,7 +97,7 @@ def test_warp_tiles_izhikevich_current_short_last_tile(ctx):
     steps = 50
     cur = thalamic(n, int(0.8 * n), steps, seed=4)
     net = sz.Network(ctx, n, 0, 8, pops, csr=csr, state=st, acc_mode=L.ACC_FIXED, graph_chunk=25)
-    net.set_update_tiles(1, 2)
+    net.set_update_tiles(mode, 2 if mode == 1 else 0)
     dcur = ctx.upload(cur)
     raster = ctx.buffer(steps * net.words * 4)
     net.run_device(steps, current_ptr=dcur.ptr, raster_ptr=raster.ptr)
@@ -108,7 +114,8 @@ def test_warp_tiles_izhikevich_current_short_last_tile(ctx):
     net.close()
 
 
-def test_warp_tiles_population_boundaries_inside_tiles(ctx):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_warp_tiles_population_boundaries_inside_tiles(ctx, mode):
     """Three populations whose boundaries fall inside warp tiles: those tiles
     take the generic per-unit update, the others the shared-memory ring."""
     n, p, D = 60_000, 6_000, 16
@@ -119,7 +126,7 @@ def test_warp_tiles_population_boundaries_inside_tiles(ctx):
     pops = [sz.Pop(pops[0].model, 0, cut, pops[0].params), sz.Pop(pops[0].model, cut, n, pv2), pops[1]]
     net = sz.Network(ctx, n, p, D, pops, state=st, acc_mode=L.ACC_FIXED, graph_chunk=25)
     net.generate(blocks, seed=78)
-    net.set_update_tiles(1, 2)
+    net.set_update_tiles(mode, 2 if mode == 1 else 0)
     on = oracle.OracleNet(n, p, D, pops, oracle.generate(blocks, 78, n + p, D), state=st)
     r = net.run(60)
     ro, ev = on.run(60, acc_mode=oracle.ACC_FIXED)
@@ -143,10 +150,12 @@ def test_warp_tiles_switch_mid_run_and_float_dyadic(ctx):
     parts = [net.run(30)]
     net.set_update_tiles(1, 2)
     parts.append(net.run(30))
+    net.set_update_tiles(2, 0)
+    parts.append(net.run(30))
     net.set_update_tiles(0, 0)
     parts.append(net.run(30))
     r = np.concatenate(parts)
-    ro, ev = on.run(90)
+    ro, ev = on.run(120)
     assert _spikes(ro) > 1000
     assert np.array_equal(r, ro)
     for k in range(4):
