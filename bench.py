@@ -82,6 +82,11 @@ def parse(argv=None):
                     help="fixed launch shape 'order,mode,group,blocks,update_block[,tiles,per_sm]' (order: "
                          "overlapped|classic; tiles 0 block tiles, 1 persistent warp tiles with per_sm update "
                          "blocks per SM) instead of the tuner")
+    ap.add_argument("--resident", default="auto", choices=["auto", "on", "off"],
+                    help="resident stepping (one cooperative launch per 100-step chunk, neuron state in shared "
+                         "memory): auto keeps it when its live step time beats the tuned graphs'")
+    ap.add_argument("--resident-warps", default="12,16,20,24",
+                    help="update warps per block the resident choice tries")
     ap.add_argument("--e2e-steps", type=int, default=2000)
     ap.add_argument("--profile-steps", type=int, default=200)
     ap.add_argument("--cpu-neurons", type=int, default=None,
@@ -93,6 +98,8 @@ def parse(argv=None):
     ap.add_argument("--batch-steps", type=int, default=1000)
     ap.add_argument("--bptt-scale", type=float, default=1.0)
     ap.add_argument("--bptt-steps", type=int, default=500)
+    ap.add_argument("--bptt-trajectory", default="auto", choices=["auto", "keep", "recompute"],
+                    help="keep the forward's membrane trajectory for the backward, or recompute it from checkpoints")
     return ap.parse_args(argv)
 
 
@@ -420,7 +427,8 @@ def bench_bptt(args):
     x = P.poisson_bits(T, Bt, rates, 1.0, 0)
     v0 = torch.zeros((Bt, N), device=dev)
     labels = torch.randint(0, K, (Bt,), generator=g).to(dev)
-    net = P.LIFCurrExpRNN(N, M, K, rp, col, beta=10.0, checkpoint_every=50)
+    net = P.LIFCurrExpRNN(N, M, K, rp, col, beta=10.0, checkpoint_every=50,
+                          store_trajectory={"auto": None, "keep": True, "recompute": False}[args.bptt_trajectory])
     for t in (w_in, val, w_out):
         t.requires_grad_(True)
 
@@ -452,11 +460,20 @@ def bench_bptt(args):
     f_ms = e[0].elapsed_time(e[1]) / reps
     fb_ms = e[1].elapsed_time(e[2]) / reps
     rate = float(P.unpack_bits(out["spikes"], N).float().mean()) * 1e3
+    stored = net.stores_trajectory(T, Bt, dev)
+    net.phase_ms = np.zeros(4)  # one more backward, timed per phase (untimed above)
+    fwdbwd()
+    torch.cuda.synchronize()
+    phases = {k: round(float(v), 3) for k, v in zip(P.BACKWARD_PHASES, net.phase_ms)}
+    net.phase_ms = None
     return {"metric": "BPTT forward+backward cost / forward cost", "fwd_ms": f_ms, "fwd_bwd_ms": fb_ms,
             "ratio": fb_ms / f_ms, "rate_hz": rate, "loss": float(loss.detach()), "trials": Bt, "steps": T,
             "neurons": N, "inputs": M, "readouts": K, "synapses": int(col.numel()), "w_in_scale": args.bptt_scale,
+            "stored_trajectory": stored, "backward_phase_ms": phases,
             "workload": "IF_curr_exp RNN 10,000 neurons (10 % recurrent), 700 Poisson inputs, 20 readouts, "
-                        "batch 64, 500 steps, fast-sigmoid slope 10, checkpoints every 50 steps"}
+                        "batch 64, 500 steps, fast-sigmoid slope 10, "
+                        + ("membrane trajectory kept by the forward for the backward" if stored
+                           else "checkpoints every 50 steps, recomputed in the backward")}
 
 
 def run_reference(args, rank):
@@ -481,6 +498,37 @@ def run_reference(args, rank):
             "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def choose_resident(net, ctx, mode, warps, steps=1000, warm=200):
+    """Live device time per step (CUDA events around szsnn_net_run_device)
+    of the tuned graphs and of resident stepping with each update-warp split;
+    resident stepping stays on when it is faster (mode "auto") or always
+    (mode "on", with its fastest split).  The network advances meanwhile:
+    this is warm-up."""
+    def live():
+        net.run_device(warm)
+        ctx.sync()
+        net.run_device(steps)
+        ctx.sync()
+        return net.device_ms() / steps * 1e3
+
+    net.set_resident(False)
+    trials = {"graphs": round(live(), 3)}
+    best = None
+    for uw in warps:
+        try:
+            net.set_resident(True, uw)
+        except Exception as e:  # the network does not qualify: graphs only
+            trials[f"resident_{uw}"] = f"refused: {e}"
+            break
+        us = live()
+        trials[f"resident_{uw}"] = round(us, 3)
+        if best is None or us < best[0]:
+            best = (us, uw)
+    on = best is not None and (mode == "on" or best[0] < trials["graphs"])
+    net.set_resident(on, best[1] if on else 0)
+    return {"resident": on, "update_warps": best[1] if on else None, "live_us": trials}
 
 
 def reduce_replicas(dist, t, units):
@@ -557,15 +605,20 @@ def main():
         ch = tune(net, replays=50, use_cache=False)
         tuning = {k: ch[k] for k in ("overlap", "mode", "group", "blocks", "update_block", "step_us",
                                      "classic_step_us")}
+    resident = None
+    if args.resident != "off" and net.overlap:
+        resident = choose_resident(net, ctx, args.resident, [int(x) for x in args.resident_warps.split(",") if x])
     net.run_device(W * S)
     ctx.sync()
     overlap = bool(net.overlap)
+    res_on = bool(resident and resident["resident"])
     s0 = net.stats()
     barrier()
     ctx.sync()
     # timed: K x S simulation steps in CUDA graphs (every graph already
-    # instantiated: szsnn_net_run_device builds them before its first event);
-    # CUDA events on the net's stream around the launches
+    # instantiated: szsnn_net_run_device builds them before its first event)
+    # or in resident chunks (one cooperative launch per 100 steps); CUDA
+    # events on the net's stream around the launches
     with ClockSampler(local_rank) as clk:
         t_wall = time.perf_counter()
         net.run_device(K * S)
@@ -619,11 +672,12 @@ def main():
     # delivery of the next step) in the overlapped order; its live time per
     # launch is the timed region's time per simulation step
     traffic = (int(NCU_STEP_TRAFFIC_FANOUT100 + max(0.0, ev_step - NCU_STEP_EVENTS_FANOUT100) * 8)
-               if (n + p == 1_100_000 and overlap) else None)
+               if (n + p == 1_100_000 and overlap and not res_on) else None)
     achieved = step_bytes / (us_live * 1e-6) / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "traffic": traffic,
-                "kernel": "k_step" if overlap else "k_propagate + k_update", "peak_source": peak_kind,
+                "kernel": "k_resident" if res_on else ("k_step" if overlap else "k_propagate + k_update"),
+                "peak_source": peak_kind,
                 "us_per_launch": round(us_live, 3), "algorithmic_bytes_per_launch": int(step_bytes),
                 "timing": "live: the timed region's device time per simulation step",
                 "l2_gbs_peak": round(chip["l2_copy_gbs"], 1),
@@ -633,6 +687,7 @@ def main():
                 "ceilings": "l2_gbs_peak: L2-resident copy of 2 x 16 MB; atomic_per_s_peak: random fp32 red into "
                             "2 x N floats (szsnn_probe_peaks, this device, this run)",
                 "replays": {"step_us": round(step_us, 3), "order": "overlapped" if overlap else "classic",
+                            "of": "the per-step launches (k_step) on scratch state" if res_on else "the timed kernels",
                             "delivery_alone_us": round(prop_us, 3), "delivery_events": ev_launch,
                             "delivery_gbs": round(ev_launch * BYTES_PER_EVENT / (prop_us * 1e-6) / 1e9, 1),
                             "delays": "2..64" if overlap else "1..64",
@@ -670,7 +725,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": headline_config(n, p, D, n_syn, args.acc),
             "parallelism": f"replicas x{world}", "step_order": "overlapped" if overlap else "classic",
-            "graph_chunk": 100, "tuning": tuning,
+            "graph_chunk": 100, "tuning": tuning, "resident": resident,
             "neuron_updates_per_s": (n + p) * sim_steps * world / (ms_max / 1e3),
             "mean_rate_hz": spikes / max(n + p, 1) / (sim_steps * DT_MS * 1e-3),
             "events_per_step": events / sim_steps,
@@ -681,7 +736,8 @@ def main():
             "e2e": {"value": e2e_tot / e2e_max, "unit": UNIT, "steps": e2e_steps,
                     "h2d_bytes_per_step": int(words * 4), "d2h_bytes_per_step": int(words * 4),
                     "api": "szsnn_net_run (forced-spike words in, raster out, page-locked host arrays)"},
-            "gpu_launches": int((1 if overlap else 2) * sim_steps + (sim_steps + 99) // 100),
+            "gpu_launches": int((sim_steps + 99) // 100 if res_on
+                                else (1 if overlap else 2) * sim_steps + (sim_steps + 99) // 100),
             "clocks": clk.summary(),
             "configs": configs,
             "batched": batched,

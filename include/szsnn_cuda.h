@@ -365,6 +365,22 @@ int szsnn_net_set_tuning(szsnn_net* net, int propagate_mode, int group, int prop
  * blocks as stay resident (blocks_per_sm, or 0 = from the occupancy of the
  * launch).  Results are identical in every mode. */
 int szsnn_net_set_update_tiles(szsnn_net* net, int mode, int blocks_per_sm);
+/* Resident stepping (on = 1): szsnn_net_run / szsnn_net_run_device run each
+ * chunk as one cooperative launch of `blocks` blocks (0 = one per SM) of
+ * 1024 threads that keeps the neurons' state in shared memory across the
+ * chunk's steps, with a bounded grid barrier between steps; in each block
+ * `update_warps` warps (0 = 16) update its neuron and source words while the
+ * other warps take their share of the far delivery.  Same step order,
+ * arithmetic and results as the overlapped graphs (bit-identical in
+ * fixed-point accumulation).  Needs the overlapped order, at most four
+ * populations with shared parameters (IF_curr_exp, IF_cond_exp, Izhikevich
+ * neurons; Poisson sources), no state monitor, and a block's neuron state
+ * within shared memory (about 1.6M IF neurons on one B200); otherwise
+ * SZSNN_ERR_ARG with the reason, and a later run whose network no longer
+ * qualifies fails with SZSNN_ERR_STATE.  szsnn_net_step and the profiling
+ * calls keep the per-step launches.  A grid barrier that waits past its
+ * bound records device error SZSNN_DEV_WAIT_TIMEOUT and ends the launch. */
+int szsnn_net_set_resident(szsnn_net* net, int on, int update_warps, int blocks);
 /* Step order.  1 (default): overlapped -- input buffers double-buffered by
  * step parity, delivery of delays >= 2 into step t+1 runs in the same launch
  * as update(t), and update(t) delivers the delay-1 bucket of its own
@@ -382,8 +398,11 @@ int szsnn_net_set_overlap(szsnn_net* net, int overlap);
  * recurrent spikes one step later; y_t = alpha y_{t-1} + Wout^T s_t, outputs
  * ymax = max_t y_t (with its first argmax) and vsum = sum_t v_t.  The
  * backward is exact except dH/du, replaced by 1/(1 + beta|u - v_thresh|)^2
- * (beta <= 0: 0), with forward spikes kept and u recomputed from checkpoints
- * every `checkpoint_every` steps.  All pointers are device pointers owned by
+ * (beta <= 0: 0), with forward spikes kept.  The backward reads u from the
+ * trajectory the forward stored in u_trace when the caller passes it again
+ * (T*B*N floats: 1.28 GB at T 500, B 64, N 10,000), else recomputes u from
+ * the checkpoints every `checkpoint_every` steps (the same kernel, so the
+ * same u and gradients bit for bit).  All pointers are device pointers owned by
  * the caller (e.g. torch tensors); `workspace` holds
  * szsnn_bptt_workspace_bytes bytes.  Calls are asynchronous on `stream`. */
 typedef struct {
@@ -404,7 +423,8 @@ typedef struct {
     float* ymax;                                    /* [B][K] out */
     int32_t* tmax;                                  /* [B][K] out */
     float* vsum;                                    /* [B][N] out */
-    float* u_trace;                                 /* [T][B][N] out: pre-reset membrane, or NULL */
+    float* u_trace;                                 /* [T][B][N] forward out: pre-reset membrane, or NULL;
+                                                       backward in: that trajectory (no recompute), or NULL */
     const float* g_ymax;                            /* [B][K] dL/dymax (backward), or NULL */
     const float* g_vsum;                            /* [B][N] dL/dvsum (backward), or NULL */
     float* dw_in;                                   /* [M][N] out (backward) */

@@ -574,19 +574,29 @@ extern "C" int szsnn_bptt_backward(const szsnn_bptt_desc* d, char* err, size_t e
     const dim3 grid_step((unsigned)sz_div_up(d->N, BP_BLOCK * BP_NPT), (unsigned)d->B);
     const dim3 grid((unsigned)sz_div_up(d->N, BP_BLOCK), (unsigned)d->B);
     const dim3 grid_in((unsigned)sz_div_up(d->N, BP_BLOCK), (unsigned)sz_div_up(d->M, DWIN_J));
-    const int nseg = (d->T + d->checkpoint_every - 1) / d->checkpoint_every;
+    // The membrane trajectory the forward stored (u_trace, [T][B][N]) is one
+    // segment read in place; otherwise each checkpoint segment is recomputed
+    // into u_seg first (the same kernel, so the same u bit for bit).
+    const bool stored = d->u_trace != nullptr;
+    if (stored) k.u_seg = d->u_trace;
+    const int seg_len = stored ? d->T : d->checkpoint_every;
+    const int nseg = (d->T + seg_len - 1) / seg_len;
     for (int seg = nseg - 1; seg >= 0; --seg) {
-        const int t0 = seg * d->checkpoint_every, t1 = std::min(d->T, t0 + d->checkpoint_every);
-        const float* c = d->ckpt + (size_t)seg * 3 * BN;
-        BP_TRY(cudaMemcpyAsync(k.Ie, c, BN * 4, cudaMemcpyDeviceToDevice, st));
-        BP_TRY(cudaMemcpyAsync(k.Ii, c + BN, BN * 4, cudaMemcpyDeviceToDevice, st));
-        BP_TRY(cudaMemcpyAsync(k.v, c + 2 * BN, BN * 4, cudaMemcpyDeviceToDevice, st));
-        pt.mark(-1);
-        for (int t = t0; t < t1; ++t) {  // recompute u_t from the checkpoint, spikes kept
-            k_bptt_step<<<grid_step, BP_BLOCK, smem, st>>>(k, t, 1, t0);
-            BP_TRY(cudaGetLastError());
+        const int t0 = seg * seg_len, t1 = std::min(d->T, t0 + seg_len);
+        if (!stored) {
+            const float* c = d->ckpt + (size_t)seg * 3 * BN;
+            BP_TRY(cudaMemcpyAsync(k.Ie, c, BN * 4, cudaMemcpyDeviceToDevice, st));
+            BP_TRY(cudaMemcpyAsync(k.Ii, c + BN, BN * 4, cudaMemcpyDeviceToDevice, st));
+            BP_TRY(cudaMemcpyAsync(k.v, c + 2 * BN, BN * 4, cudaMemcpyDeviceToDevice, st));
+            pt.mark(-1);
+            for (int t = t0; t < t1; ++t) {  // recompute u_t from the checkpoint, spikes kept
+                k_bptt_step<<<grid_step, BP_BLOCK, smem, st>>>(k, t, 1, t0);
+                BP_TRY(cudaGetLastError());
+            }
+            pt.mark(0);
+        } else {
+            pt.mark(-1);
         }
-        pt.mark(0);
         for (int t = t1 - 1; t >= t0; --t) {
             const int par = t & 1;  // buffers of step t; step t+1 uses the other parity
             const bool have_R = t < d->T - 1;

@@ -31,8 +31,10 @@
 //    selectable and is what the allocation-free single step uses.
 #include "common.cuh"
 
+#include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <tuple>
 
 // slots 0..11 as szsnn_pop_desc; 12, 13 = 1 - 1/tau_syn_E, 1 - 1/tau_syn_I
@@ -153,6 +155,10 @@ struct szsnn_net {
     double t_prop_ms = 0, t_upd_ms = 0, t_total_ms = 0;
     cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;  // around the last szsnn_net_run*
     bool run_timed = false;
+    // resident stepping: one cooperative launch per chunk, neuron state in shared memory
+    bool resident = false;
+    int res_uw = 16, res_blocks = 0;     // update warps per block, blocks (0: one per SM)
+    unsigned int* d_res_sync = nullptr;  // grid-barrier arrivals and abort flag
 };
 
 namespace {
@@ -367,31 +373,18 @@ __host__ __device__ __forceinline__ size_t far_window_bytes(int block_threads)
     return (size_t)(block_threads / 32) * 32 * FAR_WPL * sizeof(int2);
 }
 
-// Warp-flattened delivery: lanes 0..IPW-1 each resolve one (delay, spike)
-// work item to its bucket segment; the warp then walks the concatenation of
-// those segments in windows of 32 * FAR_WPL synapses.  Each item lane issues
-// asynchronous 8-byte copies of its segment's part of the window into the
-// warp's shared-memory slice and waits for them; after a warp barrier every
-// lane delivers FAR_WPL entries of the window: one memory round trip per
-// window rather than one per few loads, with no registers holding the loads
-// in flight.
-// Dynamic shared memory: far_window_bytes(blockDim.x).
-template <int IPW>
-__device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int m_lo, uint32_t pf, int blk, int nblk)
+// The warp's share of the flattened items of step t (s_pre: the scan of
+// the ring counts by delay): warp gw of nw takes items gw * IPW + k * nw * IPW
+// onward.  Returns the synapses it delivered.  CG: ring ids read through L2
+// only (a launch that also appends to the ring it reads).
+template <int IPW, bool CG>
+__device__ __forceinline__ uint32_t flat_items(const NetDev& nd, long long t, const uint32_t* s_pre, int64_t gw,
+                                               int64_t nw, int2* win, const InBuf& buf)
 {
-    __shared__ uint32_t s_pre[1025];
-    __shared__ unsigned long long s_ev;
-    extern __shared__ __align__(128) unsigned char upd_smem[];
-    const long long t = *nd.clock + k_off;
     const int D = nd.D, R = D + 1;
-    propagate_prologue(nd, t, m_lo, pf, s_pre, &s_ev, blk == 0);
-    const InBuf buf = in_buf(nd, t);
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t total = s_pre[D];
-    const int64_t gw = ((int64_t)blk * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)nblk * blockDim.x) >> 5;
     const int2* __restrict__ syn = nd.syn;
-    int2* const win = reinterpret_cast<int2*>(upd_smem) + (size_t)(threadIdx.x >> 5) * 32 * FAR_WPL;
     uint32_t ev = 0;
     for (int64_t base = gw * IPW; base < (int64_t)total; base += nw * IPW) {
         const int64_t item = base + lane;
@@ -406,7 +399,8 @@ __device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int 
             }
             const int m = lo;
             const uint32_t j = (uint32_t)(item - s_pre[m - 1]);
-            s = __ldg(&nd.ring_ids[((t - m) % R) * nd.U + j]);
+            const int32_t* rid = &nd.ring_ids[((t - m) % R) * nd.U + j];
+            s = CG ? __ldcg(rid) : __ldg(rid);
             mm = m;
         }
         // the delay-major index when most of the warp's items are consecutive
@@ -442,6 +436,31 @@ __device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int 
             __syncwarp();
         }
     }
+    return ev;
+}
+
+// Warp-flattened delivery: lanes 0..IPW-1 each resolve one (delay, spike)
+// work item to its bucket segment; the warp then walks the concatenation of
+// those segments in windows of 32 * FAR_WPL synapses.  Each item lane issues
+// asynchronous 8-byte copies of its segment's part of the window into the
+// warp's shared-memory slice and waits for them; after a warp barrier every
+// lane delivers FAR_WPL entries of the window: one memory round trip per
+// window rather than one per few loads, with no registers holding the loads
+// in flight.
+// Dynamic shared memory: far_window_bytes(blockDim.x).
+template <int IPW>
+__device__ __forceinline__ void propagate_flat(const NetDev& nd, int k_off, int m_lo, uint32_t pf, int blk, int nblk)
+{
+    __shared__ uint32_t s_pre[1025];
+    __shared__ unsigned long long s_ev;
+    extern __shared__ __align__(128) unsigned char upd_smem[];
+    const long long t = *nd.clock + k_off;
+    propagate_prologue(nd, t, m_lo, pf, s_pre, &s_ev, blk == 0);
+    const InBuf buf = in_buf(nd, t);
+    const int64_t gw = ((int64_t)blk * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)nblk * blockDim.x) >> 5;
+    int2* const win = reinterpret_cast<int2*>(upd_smem) + (size_t)(threadIdx.x >> 5) * 32 * FAR_WPL;
+    const uint32_t ev = flat_items<IPW, false>(nd, t, s_pre, gw, nw, win, buf);
     propagate_epilogue(nd, t, pf, ev, &s_ev);
 }
 
@@ -542,10 +561,11 @@ __device__ __forceinline__ void update_spikes(const NetDev& nd, long long t, int
 // events of step t's buffer moved from pending to consumed.
 __device__ __forceinline__ void step_bookkeeping(const NetDev& nd, long long t)
 {
+    // L2 loads: a resident launch reads counters other blocks wrote in it
     const int R = nd.D + 1;
-    if (t >= 1) atomicAdd(&nd.stats[1], (unsigned long long)nd.ring_cnt[(t - 1) % R]);
+    if (t >= 1) atomicAdd(&nd.stats[1], (unsigned long long)__ldcg(&nd.ring_cnt[(t - 1) % R]));
     nd.ring_cnt[(t + 1) % R] = 0;
-    const unsigned long long pend = nd.stats[2 + (t & 1)];
+    const unsigned long long pend = __ldcg(&nd.stats[2 + (t & 1)]);
     nd.stats[2 + (t & 1)] = 0;
     atomicAdd(&nd.stats[0], pend);
 }
@@ -1261,6 +1281,345 @@ __global__ void __launch_bounds__(256) k_inject(const __grid_constant__ NetDev n
     }
 }
 
+// ---- resident stepping
+//
+// One cooperative launch runs a whole chunk of overlapped steps with the
+// neurons' state held in shared memory across the steps.  One block per SM,
+// each owning a contiguous range of neuron words and one of source words
+// (word-aligned, so every raster word has one writer).  Per step t the
+// block's first `uw` warps update its units (inputs read through L2 and
+// cleared, state from and to shared memory, the spike epilogue of the tile
+// update: ring append, raster word, delay-1 delivery into step t+1); its
+// other warps take their share of the far delivery into step t+1 (delays
+// >= 2, ring slots <= t-1), split over the delivery warps of all blocks.  A
+// bounded grid barrier ends the step: update(t+1) needs every delivery into
+// step t+1 and every ring append of step t.  Per step a neuron moves only its
+// inputs through L2 (read and clear), not its state.  Data written inside
+// the launch (ring counts and ids, inputs, statistics) is read with L2 loads.
+struct ResSync {
+    unsigned int count;  // arrivals: one per block per step
+    unsigned int abort;  // set by a block whose wait ran out
+};
+
+struct ResRange {
+    int64_t n_lo, n_cnt;  // neuron words of the block, as unit ids (32 per word)
+    int64_t s_lo, s_cnt;  // source words (those after the word holding the last neuron)
+};
+
+__host__ __device__ __forceinline__ ResRange res_range(int64_t N, int64_t words, int b, int nb)
+{
+    const int64_t nw = sz_div_up(N, 32), sw = words - nw;
+    const int64_t a0 = nw * b / nb, a1 = nw * (b + 1) / nb;
+    const int64_t c0 = nw + sw * b / nb, c1 = nw + sw * (b + 1) / nb;
+    return ResRange{32 * a0, 32 * (a1 - a0), 32 * c0, 32 * (c1 - c0)};
+}
+
+// neuron slots of a block's shared state: its largest neuron range
+__host__ __device__ __forceinline__ int64_t res_cap(int64_t N, int nb) { return 32 * sz_div_up(sz_div_up(N, 32), nb); }
+
+#define RES_THREADS 1024
+#define RES_UB 4                 // units per update thread in flight (loads issued together)
+#define RES_WAIT_ITERS (1 << 21)  // grid-barrier polls before a block gives up (about a second)
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void named_sync(int id, int threads)
+{
+    asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(threads) : "memory");
+}
+
+// Bounded grid barrier.  Thread 0 first adds the block's delivered events of
+// the step to the pending counter of step t+1, then arrives and polls; every
+// write of the block before the barrier is visible to every block after it.
+// Returns false when a wait ran out here or in another block (device error 7
+// is recorded): the kernel then stops stepping.
+__device__ __forceinline__ bool res_grid_sync(const NetDev& nd, ResSync* s, unsigned int target, int* s_flag,
+                                              unsigned long long* s_ev, unsigned long long* pending)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (*s_ev) { atomicAdd(pending, *s_ev); *s_ev = 0; }
+        __threadfence();
+        atomicAdd(&s->count, 1u);
+        int ok = 0;
+        for (int i = 0; i < RES_WAIT_ITERS; ++i) {
+            if (ld_acquire_u32(&s->count) >= target) { ok = 1; break; }
+            if (*reinterpret_cast<volatile unsigned int*>(&s->abort)) break;
+            if (i >= 16) __nanosleep(64);
+        }
+        if (!ok) {
+            atomicExch(&s->abort, 1u);
+            dev_error(nd.err, SZSNN_DEV_WAIT_TIMEOUT, target);
+        }
+        __threadfence();
+        *s_flag = ok;
+    }
+    __syncthreads();
+    return *s_flag != 0;
+}
+
+// One population's parameters in registers (constant slot indices; the
+// slots a model does not read are never loaded)
+struct RegParams {
+    float p[POP_SLOTS];
+    __device__ __forceinline__ float operator()(int k) const { return p[k]; }
+};
+
+// A batch of RES_UB units per thread, all in population P of neuron model
+// MODEL (warp-uniform): state loads from shared memory for every unit first,
+// then the model arithmetic on registers (independent units, so their
+// instruction chains interleave), then the stores.  Arithmetic as
+// tile_unit's; act[u]: the unit is updated; id[u] - n_lo: its shared-memory
+// slot.
+template <int MODEL>
+__device__ __forceinline__ void res_batch(const PopDev& P, float* const* st, const InBuf& inb, bool fixed,
+                                          const uint32_t* id, uint32_t n_lo, const bool* act, const float* in_e,
+                                          const float* in_i, const float* ext, const bool* f, bool* spk)
+{
+    RegParams rp;
+#pragma unroll
+    for (int k = 0; k < POP_SLOTS; ++k) rp.p[k] = P.p[k];
+    const bool half = (P.flags & SZSNN_POP_IZH_HALF_STEPS) != 0;
+    float v[RES_UB], g1[RES_UB], g2[RES_UB], fr[RES_UB];
+#pragma unroll
+    for (int u = 0; u < RES_UB; ++u) {
+        v[u] = g1[u] = g2[u] = fr[u] = 0.0f;
+        if (act[u]) {
+            v[u] = st[0][(id[u] - n_lo)];
+            g1[u] = st[1][(id[u] - n_lo)];
+            if (MODEL != SZSNN_IZHIKEVICH) { g2[u] = st[2][(id[u] - n_lo)]; fr[u] = st[3][(id[u] - n_lo)]; }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < RES_UB; ++u) {
+        bool s;
+        if (MODEL == SZSNN_IF_CURR_EXP)
+            s = sz_if_curr_exp(rp, v[u], g1[u], g2[u], fr[u], in_e[u], in_i[u], ext[u], f[u], rp(12), rp(13));
+        else if (MODEL == SZSNN_IF_COND_EXP)
+            s = sz_if_cond_exp(rp, v[u], g1[u], g2[u], fr[u], in_e[u], in_i[u], ext[u], f[u], rp(12), rp(13));
+        else
+            s = sz_izhikevich(rp, v[u], g1[u], in_e[u], in_i[u], ext[u], f[u], half);
+        spk[u] = act[u] && s;
+    }
+#pragma unroll
+    for (int u = 0; u < RES_UB; ++u) {
+        if (!act[u]) continue;
+        st[0][(id[u] - n_lo)] = v[u];
+        st[1][(id[u] - n_lo)] = g1[u];
+        if (MODEL != SZSNN_IZHIKEVICH) { st[2][(id[u] - n_lo)] = g2[u]; st[3][(id[u] - n_lo)] = fr[u]; }
+        if (fixed) { inb.fe[id[u]] = 0; inb.fi[id[u]] = 0; }
+        else { inb.e[id[u]] = 0.0f; inb.i[id[u]] = 0.0f; }
+    }
+}
+
+// The update warps' units of step t: the block's neuron ids, then its source
+// ids, RES_UB per thread at a time (the batch's loads in flight together);
+// warp w's lanes hold 32 consecutive ids, one raster word.  A batch whose
+// active units all lie in one population (warp-uniform) runs that model's
+// batch update; others run unit by unit.  Arithmetic and side effects as the
+// generic update's (update_generic), with the state in shared memory slot
+// id - n_lo.  Ids fit 32 bits (resident networks hold a few million units).
+template <bool FIXED>
+__device__ __forceinline__ void res_update(const NetDev& nd, const PopDev* __restrict__ sp, const ResRange& rr,
+                                           float* const* st, long long t, const uint32_t* __restrict__ forced,
+                                           const float* __restrict__ current, uint32_t* __restrict__ out_words,
+                                           int nthr, bool all_owned)
+{
+    const InBuf inb = in_buf(nd, t);
+    const uint32_t lane = threadIdx.x & 31, wbase = threadIdx.x & ~31u;
+    const uint32_t n_lo = (uint32_t)rr.n_lo, n_cnt = (uint32_t)rr.n_cnt, s_lo = (uint32_t)rr.s_lo;
+    const uint32_t total = (uint32_t)(rr.n_cnt + rr.s_cnt);  // a multiple of 32
+    const uint32_t N = (uint32_t)nd.N, U = (uint32_t)nd.U;
+    const int np = nd.npops;
+    for (uint32_t i0 = 0; i0 < total; i0 += (uint32_t)nthr * RES_UB) {
+        uint32_t id[RES_UB];
+        float in_e[RES_UB], in_i[RES_UB], ext[RES_UB];
+        bool f[RES_UB], act[RES_UB], spk[RES_UB];
+        int pi[RES_UB];
+#pragma unroll
+        for (int u = 0; u < RES_UB; ++u) {
+            const uint32_t i = i0 + (uint32_t)u * nthr + threadIdx.x;
+            id[u] = i < n_cnt ? n_lo + i : s_lo + (i - n_cnt);
+            in_e[u] = in_i[u] = ext[u] = 0.0f;
+            f[u] = false;
+            act[u] = i < total && id[u] < U && (all_owned || owned(nd, id[u]));
+            pi[u] = -1;
+            if (!act[u]) continue;
+            for (int k = 0; k < np; ++k)
+                if (id[u] >= sp[k].begin && id[u] < sp[k].end) pi[u] = k;
+            if (pi[u] < 0) act[u] = false;
+            if (act[u] && id[u] < N) {
+                if (FIXED) {
+                    in_e[u] = __ll2float_rn(__ldcg(&inb.fe[id[u]])) * (1.0f / 4294967296.0f);
+                    in_i[u] = __ll2float_rn(__ldcg(&inb.fi[id[u]])) * (1.0f / 4294967296.0f);
+                } else {
+                    in_e[u] = __ldcg(&inb.e[id[u]]);
+                    in_i[u] = __ldcg(&inb.i[id[u]]);
+                }
+                if (current) ext[u] = current[id[u]];
+            }
+            if (forced && act[u]) f[u] = ((forced[id[u] >> 5] >> (id[u] & 31)) & 1u) != 0u;
+        }
+        // the batch's population when every active unit of the warp lies in one
+        int mine = -2;
+        bool uni = true;
+#pragma unroll
+        for (int u = 0; u < RES_UB; ++u)
+            if (act[u]) {
+                if (mine == -2) mine = pi[u];
+                else if (pi[u] != mine) uni = false;
+            }
+        const int p0 = __reduce_max_sync(0xffffffffu, mine);
+        uni = __all_sync(0xffffffffu, uni && (mine == -2 || mine == p0)) && p0 >= 0;
+        if (uni) {
+            const PopDev& P = sp[p0];
+            if (P.model == SZSNN_IF_COND_EXP)
+                res_batch<SZSNN_IF_COND_EXP>(P, st, inb, FIXED, id, n_lo, act, in_e, in_i, ext, f, spk);
+            else if (P.model == SZSNN_IF_CURR_EXP)
+                res_batch<SZSNN_IF_CURR_EXP>(P, st, inb, FIXED, id, n_lo, act, in_e, in_i, ext, f, spk);
+            else if (P.model == SZSNN_IZHIKEVICH)
+                res_batch<SZSNN_IZHIKEVICH>(P, st, inb, FIXED, id, n_lo, act, in_e, in_i, ext, f, spk);
+            else {
+#pragma unroll
+                for (int u = 0; u < RES_UB; ++u)
+                    spk[u] = act[u] && (sz_poisson_fires(P.seed, (int64_t)id[u] - P.begin, t, P.p[0]) || f[u]);
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < RES_UB; ++u) {
+                spk[u] = false;
+                if (!act[u]) continue;
+                const PopDev& P = sp[pi[u]];
+                if (id[u] < N) {
+                    float v = st[0][(id[u] - n_lo)], g1 = st[1][(id[u] - n_lo)], g2 = 0.0f, fr = 0.0f;
+                    if (P.model != SZSNN_IZHIKEVICH) { g2 = st[2][(id[u] - n_lo)]; fr = st[3][(id[u] - n_lo)]; }
+                    spk[u] = run_neuron(SharedParams{P.p}, P.model, P.flags, v, g1, g2, fr, in_e[u], in_i[u], ext[u],
+                                        f[u]);
+                    st[0][(id[u] - n_lo)] = v;
+                    st[1][(id[u] - n_lo)] = g1;
+                    if (P.model != SZSNN_IZHIKEVICH) { st[2][(id[u] - n_lo)] = g2; st[3][(id[u] - n_lo)] = fr; }
+                    if (FIXED) { inb.fe[id[u]] = 0; inb.fi[id[u]] = 0; }
+                    else { inb.e[id[u]] = 0.0f; inb.i[id[u]] = 0.0f; }
+                } else if (P.model == SZSNN_POISSON) {
+                    spk[u] = sz_poisson_fires(P.seed, (int64_t)id[u] - P.begin, t, P.p[0]) || f[u];
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < RES_UB; ++u) {
+            if (i0 + (uint32_t)u * nthr + wbase >= total) continue;  // warp-uniform
+            __syncwarp();
+            update_spikes(nd, t, id[u], spk[u], lane, out_words);
+        }
+    }
+}
+
+// The delivery warps' share of the far delivery into step tt (delays 2..D):
+// the ring counts scanned once per block (named barrier 1 over the delivery
+// threads), then the flattened walk with L2 loads of the ring ids.
+template <int IPW>
+__device__ __forceinline__ void res_deliver(const NetDev& nd, long long tt, int64_t gw, int64_t nw, int dtid,
+                                            int dthr, uint32_t* s_pre, int2* win, unsigned long long* s_ev,
+                                            bool book)
+{
+    const int D = nd.D, R = D + 1;
+    if (book && dtid == 0) step_bookkeeping(nd, tt - 1);  // its loads overlap the ring-count loads
+    for (int m = dtid + 1; m <= D; m += dthr) {
+        const long long tm = tt - m;
+        s_pre[m] = (m >= 2 && tm >= 0) ? __ldcg(&nd.ring_cnt[tm % R]) : 0u;
+    }
+    if (dtid == 0) s_pre[0] = 0;
+    named_sync(1, dthr);
+    if (dtid < 32) {  // inclusive scan of counts over m = 1..D
+        uint32_t carry = 0;
+        const uint32_t lane = (uint32_t)dtid;
+        for (int m0 = 1; m0 <= D; m0 += 32) {
+            const int m = m0 + (int)lane;
+            const uint32_t c = (m <= D) ? s_pre[m] : 0u;
+            uint32_t incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (uint32_t)o) incl += y;
+            }
+            if (m <= D) s_pre[m] = carry + incl;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+    }
+    named_sync(1, dthr);
+    uint32_t ev = flat_items<IPW, true>(nd, tt, s_pre, gw, nw, win, in_buf(nd, tt));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
+    if ((dtid & 31) == 0 && ev) atomicAdd(s_ev, (unsigned long long)ev);
+}
+
+// `len` overlapped steps from the step counter on; uw update warps per
+// block, nst state slots kept (2: Izhikevich only, 4 otherwise); per-step
+// forced words / currents / raster words at step k of the chunk arrays.
+// Dynamic shared memory: the delivery warps' copy windows, then nst arrays of
+// res_cap(N, gridDim.x) floats.
+template <bool FIXED, int IPW>
+__global__ void __launch_bounds__(RES_THREADS, 1)
+    k_resident(const __grid_constant__ NetDev nd, ResSync* sync, long long* clock, int len, int uw, int nst,
+               const uint32_t* __restrict__ forced, const float* __restrict__ current, uint32_t* __restrict__ raster)
+{
+    extern __shared__ __align__(128) unsigned char upd_smem[];
+    __shared__ uint32_t s_pre[1025];
+    __shared__ unsigned long long s_ev;
+    __shared__ PopDev s_pop[INLINE_POPS];
+    __shared__ int s_flag;
+    const int b = blockIdx.x, nb = gridDim.x;
+    const ResRange rr = res_range(nd.N, nd.words, b, nb);
+    const int64_t cap = res_cap(nd.N, nb);
+    const int warp = (int)(threadIdx.x >> 5), ndw = (int)(blockDim.x >> 5) - uw;
+    int2* const win = reinterpret_cast<int2*>(upd_smem);
+    float* const sb = reinterpret_cast<float*>(upd_smem + (size_t)ndw * 32 * FAR_WPL * sizeof(int2));
+    float* const st[4] = {sb, sb + cap, nst > 2 ? sb + 2 * cap : nullptr, nst > 2 ? sb + 3 * cap : nullptr};
+    float* const gst[4] = {nd.st0, nd.st1, nd.st2, nd.st3};
+    if ((int)threadIdx.x < nd.npops) s_pop[threadIdx.x] = nd.pops[threadIdx.x];
+    if (threadIdx.x == 0) s_ev = 0;
+    for (int64_t i = threadIdx.x; i < rr.n_cnt; i += blockDim.x) {
+        const int64_t id = rr.n_lo + i;
+        if (id < nd.N) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < nst) st[k][i] = gst[k][id];
+        }
+    }
+    const long long t0 = *clock;  // every block reads it before its first arrival; block 0 advances it after the last
+    const bool all_owned = nd.own_lo[0] == 0 && nd.own_hi[0] == nd.N && nd.own_lo[1] == nd.N && nd.own_hi[1] == nd.U;
+    __syncthreads();
+    for (int k = 0; k < len; ++k) {
+        const long long t = t0 + k;
+        if (warp < uw) {
+            if (b == 0 && threadIdx.x == 0 && nd.D < 2) step_bookkeeping(nd, t);
+            res_update<FIXED>(nd, s_pop, rr, st, t, forced ? forced + (size_t)k * nd.words : nullptr,
+                              current ? current + (size_t)k * (size_t)nd.N : nullptr,
+                              raster ? raster + (size_t)k * nd.words : nullptr, uw * 32, all_owned);
+        } else if (nd.D >= 2) {
+            res_deliver<IPW>(nd, t + 1, (int64_t)b * ndw + (warp - uw), (int64_t)nb * ndw,
+                             (int)threadIdx.x - uw * 32, ndw * 32, s_pre, win + (size_t)(warp - uw) * 32 * FAR_WPL,
+                             &s_ev, b == 0);
+        }
+        if (!res_grid_sync(nd, sync, (unsigned int)(nb * (k + 1)), &s_flag, &s_ev, &nd.stats[2 + ((t + 1) & 1)]))
+            break;
+    }
+    for (int64_t i = threadIdx.x; i < rr.n_cnt; i += blockDim.x) {
+        const int64_t id = rr.n_lo + i;
+        if (id < nd.N) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < nst) gst[k][id] = st[k][i];
+        }
+    }
+    if (b == 0 && threadIdx.x == 0) *clock = t0 + len;
+}
+
 // ---- device generator (fixed fan-out), one warp per row
 struct GenDev {
     int64_t src_begin, src_count, tgt_begin, tgt_count;
@@ -1622,6 +1981,100 @@ cudaError_t launch_step(szsnn_net* n, const NetDev& d, int k_off, const uint32_t
     return cudaGetLastError();
 }
 
+// ---- resident stepping (host)
+
+int res_blocks(const szsnn_net* n)
+{
+    const int64_t want = n->res_blocks > 0 ? n->res_blocks : num_sms(n->ctx);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(want, n->words));
+}
+
+template <bool FIXED>
+void* res_kernel(int ipw)
+{
+    if (ipw == 8) return (void*)k_resident<FIXED, 8>;
+    if (ipw == 32) return (void*)k_resident<FIXED, 32>;
+    return (void*)k_resident<FIXED, 16>;
+}
+
+void* res_kernel(const szsnn_net* n)
+{
+    const int ipw = n->prop_mode == 1 ? n->prop_group : 16;
+    return n->acc_mode == SZSNN_ACC_FIXED ? res_kernel<true>(ipw) : res_kernel<false>(ipw);
+}
+
+// Whether the network can step resident; on success the dynamic shared
+// memory and the state slots kept.  `why` names the first obstacle.
+bool res_check(szsnn_net* n, std::string* why, size_t* smem, int* nst)
+{
+    auto no = [&](const char* m) { if (why) *why = m; return false; };
+    if (!n->overlap) return no("resident stepping needs the overlapped step order");
+    if (n->npops > INLINE_POPS) return no("resident stepping takes at most 4 populations");
+    if (n->mon_n) return no("resident stepping does not record a state monitor");
+    if (n->res_uw < 1 || n->res_uw > RES_THREADS / 32 - 1) return no("update warps must be in 1..31");
+    if (n->U >= ((int64_t)1 << 31)) return no("resident stepping takes fewer than 2^31 units");
+    int slots = 2;
+    for (const PopDev& q : n->h_pops) {
+        const bool neuron_model = q.model == SZSNN_IF_CURR_EXP || q.model == SZSNN_IF_COND_EXP ||
+                                  q.model == SZSNN_IZHIKEVICH;
+        if (q.pn) return no("resident stepping needs shared population parameters");
+        if (q.begin < n->N && q.end > n->N) return no("a population spans neurons and sources");
+        if (q.begin < n->N && !neuron_model) return no("neurons of a source model");
+        if (q.begin >= n->N && q.model != SZSNN_POISSON) return no("sources other than Poisson");
+        if (q.model != SZSNN_IZHIKEVICH && neuron_model) slots = 4;
+    }
+    int dev = 0, coop = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return no("device attributes unavailable");
+    }
+    if (!coop) return no("the device has no cooperative launch");
+    const int nb = res_blocks(n);
+    const size_t bytes = (size_t)(RES_THREADS / 32 - n->res_uw) * 32 * FAR_WPL * sizeof(int2) +
+                         (size_t)slots * (size_t)res_cap(n->N, nb) * sizeof(float);
+    void* k = res_kernel(n);
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, k) != cudaSuccess) { cudaGetLastError(); return no("kernel attributes unavailable"); }
+    if (bytes + fa.sharedSizeBytes > (size_t)optin)
+        return no("the neuron state of a block does not fit in shared memory");
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return no("shared memory limit not accepted");
+    }
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, RES_THREADS, bytes) != cudaSuccess || occ < 1) {
+        cudaGetLastError();
+        return no("a resident block does not fit on an SM");
+    }
+    if ((int64_t)occ * num_sms(n->ctx) < nb) return no("more resident blocks than fit on the device");
+    *smem = bytes;
+    *nst = slots;
+    return true;
+}
+
+// one chunk of `len` resident steps (stage buffer b of the run's I/O);
+// smem and nst from res_check
+cudaError_t launch_resident(szsnn_net* n, int len, int flags, int b, cudaStream_t st, size_t smem, int nst)
+{
+    if (!n->d_res_sync) {
+        cudaError_t e = cudaMalloc((void**)&n->d_res_sync, sizeof(ResSync));
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = cudaMemsetAsync(n->d_res_sync, 0, sizeof(ResSync), st);
+    if (e != cudaSuccess) return e;
+    NetDev d = make_dev(n, 0);
+    ResSync* sync = reinterpret_cast<ResSync*>(n->d_res_sync);
+    long long* clock = n->d_clock;
+    const uint32_t* fw = (flags & 1) ? n->d_forced_stage[b] : nullptr;
+    const float* cu = (flags & 2) ? n->d_current_stage : nullptr;
+    uint32_t* ras = (flags & 4) ? n->d_raster_stage[b] : nullptr;
+    int uw = n->res_uw;
+    void* args[] = {&d, &sync, &clock, &len, &uw, &nst, &fw, &cu, &ras};
+    return cudaLaunchCooperativeKernel(res_kernel(n), dim3((unsigned)res_blocks(n)), dim3(RES_THREADS), args, smem, st);
+}
+
 template <class T>
 cudaError_t dalloc(T** p, size_t count)
 {
@@ -1663,6 +2116,7 @@ void free_net(szsnn_net* n)
     cudaFree(n->d_current_stage);
     cudaFree(n->d_dbg_in);
     cudaFree(n->d_inject);
+    cudaFree(n->d_res_sync);
     if (n->h_pinned_words) cudaFreeHost(n->h_pinned_words);
     for (auto& h : n->h_io) if (h) cudaFreeHost(h);
     if (n->ev_run0) cudaEventDestroy(n->ev_run0);
@@ -2136,10 +2590,18 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
             else if (left < n->chunk + edge) len = (int)(left - edge);
         }
         cudaGraphExec_t ex = nullptr;
-        int rc = net_graph(n, len, flags, (int)(k & 1), (int)((n->steps_done + done) & 1), &ex);
-        if (rc) return rc;
+        if (!n->resident) {
+            int rc = net_graph(n, len, flags, (int)(k & 1), (int)((n->steps_done + done) & 1), &ex);
+            if (rc) return rc;
+        }
         plan.emplace_back(len, ex);
         done += len;
+    }
+    size_t res_smem = 0;
+    int res_nst = 0;
+    if (n->resident) {  // checked before the run's first event, as the graphs are built
+        std::string why;
+        if (!res_check(n, &why, &res_smem, &res_nst)) return szsnn_set_error(n->ctx, SZSNN_ERR_STATE, why);
     }
     NET_TRY(n, cudaEventRecord(n->ev_run0, st));
     NET_TRY(n, cudaStreamWaitEvent(cp, n->ev_run0, 0));  // copies follow earlier work on the main stream
@@ -2175,10 +2637,15 @@ static int net_run_impl(szsnn_net* n, int64_t steps, const uint32_t* forced, con
         if (current && n->N)
             NET_TRY(n, cudaMemcpyAsync(n->d_current_stage, current + (size_t)done * n->N, (size_t)len * n->N * 4, in_kind, st));
         if (raster && k >= 2) NET_TRY(n, cudaStreamWaitEvent(st, n->ev_out[b], 0));  // stage b copied out
-        NET_TRY(n, cudaGraphLaunch(plan[k].second, st));
+        if (n->resident) {
+            NET_TRY(n, launch_resident(n, len, flags, b, st, res_smem, res_nst));
+            n->kernel_launches += 1;
+        } else {
+            NET_TRY(n, cudaGraphLaunch(plan[k].second, st));
+            n->graph_launches += 1;
+            n->kernel_launches += (uint64_t)((n->overlap ? 1 : 2) + (n->mon_n ? 1 : 0)) * len + 1;
+        }
         NET_TRY(n, cudaEventRecord(n->ev_comp[b], st));
-        n->graph_launches += 1;
-        n->kernel_launches += (uint64_t)((n->overlap ? 1 : 2) + (n->mon_n ? 1 : 0)) * len + 1;
         if (raster) {
             int rc = flush(b);  // bounce b last held chunk k-2
             if (rc) return rc;
@@ -2380,6 +2847,32 @@ extern "C" int szsnn_net_set_update_tiles(szsnn_net* n, int mode, int blocks_per
     n->upd_per_sm = blocks_per_sm;
     for (auto& kv : n->graphs) cudaGraphExecDestroy(kv.second);
     n->graphs.clear();
+    return SZSNN_OK;
+}
+
+extern "C" int szsnn_net_set_resident(szsnn_net* n, int on, int update_warps, int blocks)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    if (on != 0 && on != 1) return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "resident must be 0 or 1");
+    if (update_warps < 0 || update_warps > RES_THREADS / 32 - 1)
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "update warps must be in 0..31 (0: 16)");
+    if (blocks < 0 || blocks > 4096) return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "blocks must be in 0..4096");
+    const bool was = n->resident;
+    const int uw0 = n->res_uw, nb0 = n->res_blocks;
+    n->resident = on != 0;
+    n->res_uw = update_warps > 0 ? update_warps : 16;
+    n->res_blocks = blocks;
+    if (n->resident) {
+        std::string why;
+        size_t smem = 0;
+        int nst = 0;
+        if (!res_check(n, &why, &smem, &nst)) {
+            n->resident = was;
+            n->res_uw = uw0;
+            n->res_blocks = nb0;
+            return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, why);
+        }
+    }
     return SZSNN_OK;
 }
 

@@ -243,6 +243,15 @@ class Network:
         persistent block tiles (`blocks_per_sm`, 0: as many as stay resident)."""
         L.check(self.lib.szsnn_net_set_update_tiles(self.h, mode, blocks_per_sm), self.ctx.h, "set_update_tiles")
 
+    def set_resident(self, on: bool, update_warps: int = 0, blocks: int = 0) -> None:
+        """Resident stepping: each run chunk is one cooperative launch that
+        keeps the neurons' state in shared memory across its steps
+        (`update_warps` of each block's 32 warps update, 0: 16; `blocks`, 0:
+        one per SM).  Raises SzsnnError with the reason when the network does
+        not qualify."""
+        L.check(self.lib.szsnn_net_set_resident(self.h, 1 if on else 0, update_warps, blocks), self.ctx.h,
+                "set_resident")
+
     overlap = True
 
     def set_overlap(self, on: bool) -> None:

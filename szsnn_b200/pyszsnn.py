@@ -14,7 +14,9 @@ synaptic channel, gather_kernel.cl:172-178):
   readouts y_t = alpha y_{t-1} + w_out^T s_t; outputs ymax = max_t y_t and
   vsum = sum_t v_t.  Gradients are exact except dH/du, replaced by the fast
   sigmoid 1/(1 + beta|u - v_thresh|)^2; forward spikes are kept, and u is
-  recomputed from checkpoints every `checkpoint_every` steps.
+  recomputed from checkpoints every `checkpoint_every` steps, or read from
+  the trajectory the forward kept (store_trajectory; by default whenever it
+  fits the budget).
 """
 from __future__ import annotations
 
@@ -57,12 +59,24 @@ class LIFCurrExpRNN:
     alpha: float = 0.95
     beta: float = 10.0
     checkpoint_every: int = 50
+    # keep the membrane trajectory u [T,B,N] from the forward for the backward
+    # (no recompute): True, False, or None = when it takes at most
+    # trajectory_budget bytes and a quarter of the device's free memory
+    store_trajectory: bool | None = None
+    trajectory_budget: int = 16 << 30
     phase_ms: np.ndarray | None = field(default=None, repr=False)  # float64 [4]: backward adds its device ms
                                                                     # per phase (BACKWARD_PHASES) when set
 
     @property
     def nnz(self) -> int:
         return int(self.rec_col.numel())
+
+    def stores_trajectory(self, T: int, B: int, device) -> bool:
+        if self.store_trajectory is not None:
+            return bool(self.store_trajectory)
+        nbytes = 4 * T * B * self.n_neurons
+        free = torch.cuda.mem_get_info(device)[0]
+        return nbytes <= self.trajectory_budget and 4 * nbytes <= free
 
 
 def _ptr(t):
@@ -120,9 +134,11 @@ class LIFCurrExpFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, w_in, rec_val, w_out, x_bits, v0, net):
         tensors = [t.contiguous() for t in (w_in, rec_val, w_out, x_bits, v0)]
-        out = _forward(net, *tensors)
+        store = net.stores_trajectory(int(x_bits.shape[0]), int(v0.shape[0]), v0.device)
+        out = _forward(net, *tensors, trace_u=store)
         ctx.net = net
         ctx.ws = out["workspace"]
+        ctx.u_trace = out.get("u_trace")
         ctx.save_for_backward(*tensors, out["spikes"], out["ckpt"], out["tmax"])
         return out["ymax"], out["vsum"]
 
@@ -138,7 +154,7 @@ class LIFCurrExpFunction(torch.autograd.Function):
         g_vsum = None if g_vsum is None else g_vsum.contiguous().float()
         d = _desc(net, B, T, dict(w_in=w_in, rec_val=rec_val, w_out=w_out, x_bits=x_bits, v0=v0, spikes=spikes,
                                   ckpt=ckpt, tmax=tmax, g_ymax=g_ymax, g_vsum=g_vsum, dw_in=dw_in, dw_rec=dw_rec,
-                                  dw_out=dw_out, workspace=ctx.ws))
+                                  dw_out=dw_out, workspace=ctx.ws, u_trace=ctx.u_trace))
         if net.phase_ms is not None:
             if net.phase_ms.dtype != np.float64 or net.phase_ms.shape != (4,) or not net.phase_ms.flags.c_contiguous:
                 raise ValueError("phase_ms must be a contiguous float64 array of 4")

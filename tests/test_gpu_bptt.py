@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _setup(N=300, M=60, K=6, B=4, T=130, density=0.1, w_in_scale=0.6, w_rec_scale=1.0, beta=10.0, ck=50, seed=0,
-           shuffle_rows=False):
+           shuffle_rows=False, store=False):
     dev = torch.device("cuda")
     rp, col, val = P.random_recurrent(N, density, seed, dev)
     if shuffle_rows:  # columns out of order inside each row
@@ -39,7 +39,7 @@ def _setup(N=300, M=60, K=6, B=4, T=130, density=0.1, w_in_scale=0.6, w_rec_scal
     rates = torch.rand(M, generator=g) * 50.0
     x = P.poisson_bits(T, B, rates.to(dev), 1.0, seed)
     v0 = (torch.rand((B, N), generator=g) * 0.5).to(dev)
-    net = P.LIFCurrExpRNN(N, M, K, rp, col, alpha=0.95, beta=beta, checkpoint_every=ck)
+    net = P.LIFCurrExpRNN(N, M, K, rp, col, alpha=0.95, beta=beta, checkpoint_every=ck, store_trajectory=store)
     return net, w_in, val, w_out, x, v0
 
 
@@ -72,13 +72,17 @@ def test_forward_matches_fp64_reference():
     assert np.allclose(out["vsum"].cpu().numpy(), fw2["vsum"], rtol=1e-4, atol=1e-3)
 
 
-@pytest.mark.parametrize("ck,N,B,shuffle", [(50, 300, 4, False), (13, 300, 4, False), (50, 1000, 37, False),
-                                           (50, 3000, 64, False), (50, 300, 4, True)])
-def test_gradients_match_fp64_bptt(ck, N, B, shuffle):
+@pytest.mark.parametrize("ck,N,B,shuffle,store", [(50, 300, 4, False, False), (13, 300, 4, False, False),
+                                                 (50, 1000, 37, False, False), (50, 3000, 64, False, False),
+                                                 (50, 300, 4, True, False), (50, 300, 4, False, True),
+                                                 (50, 1000, 37, False, True)])
+def test_gradients_match_fp64_bptt(ck, N, B, shuffle, store):
     """B = 37: trials not a multiple of four (the SpMM's float4 trial groups
     are partly empty); N = 3000, B = 64: full trial groups, long rows;
-    shuffle: columns out of order inside the rows."""
-    net, w_in, val, w_out, x, v0 = _setup(ck=ck, N=N, B=B, T=130 if N <= 300 else 40, shuffle_rows=shuffle)
+    shuffle: columns out of order inside the rows; store: the backward reads
+    the trajectory the forward kept instead of recomputing it."""
+    net, w_in, val, w_out, x, v0 = _setup(ck=ck, N=N, B=B, T=130 if N <= 300 else 40, shuffle_rows=shuffle,
+                                          store=store)
     w_in.requires_grad_(True)
     val.requires_grad_(True)
     w_out.requires_grad_(True)
@@ -209,3 +213,34 @@ def test_full_size_gradients_do_not_depend_on_the_checkpoint_interval():
     assert torch.equal(grads[0][0], grads[1][0]) and torch.equal(grads[0][1], grads[1][1])
     g0, g1 = grads[0][2], grads[1][2]
     assert float((g0 - g1).abs().max()) <= 1e-6 * float(g0.abs().max())
+
+
+def test_stored_trajectory_gives_the_recomputed_gradients():
+    """The benchmark's shape over 100 steps: the backward reading the
+    trajectory the forward kept and the backward recomputing it from
+    checkpoints every 50 steps give bit-identical input and recurrent weight
+    gradients (the readout's fp32 atomics: within 1e-6 relative); with the
+    trajectory kept the recompute phase is empty."""
+    grads, phases = [], []
+    for store in (False, True):
+        net, w_in, val, w_out, x, v0 = _setup(N=10000, M=700, K=20, B=64, T=100, ck=50, seed=11, store=store)
+        net.phase_ms = np.zeros(4)
+        for t in (w_in, val, w_out):
+            t.requires_grad_(True)
+        ymax, vsum = P.LIFCurrExpFunction.apply(w_in, val, w_out, x, v0, net)
+        (ymax.sum() + 1e-3 * vsum.sum()).backward()
+        torch.cuda.synchronize()
+        grads.append([t.grad.clone() for t in (w_in, val, w_out)])
+        phases.append(net.phase_ms.copy())
+    assert torch.equal(grads[0][0], grads[1][0]) and torch.equal(grads[0][1], grads[1][1])
+    g0, g1 = grads[0][2], grads[1][2]
+    assert float((g0 - g1).abs().max()) <= 1e-6 * float(g0.abs().max())
+    assert phases[0][0] > 0 and phases[1][0] == 0
+
+
+def test_trajectory_kept_by_default_when_it_fits():
+    net, *_ = _setup(N=300, B=4, T=130)
+    net.store_trajectory = None
+    assert net.stores_trajectory(130, 4, torch.device("cuda"))
+    net.trajectory_budget = 1000
+    assert not net.stores_trajectory(130, 4, torch.device("cuda"))

@@ -5,7 +5,8 @@ the headline number is quoted on.
   * against the oracle (generated on the CPU from the same seed by the same
     algorithm, run on all host threads):
       - fixed-point accumulation: rasters, all four state slots and the event
-        count bit for bit over 100 steps, with either update tile scheme;
+        count bit for bit over 100 steps, with each update tile scheme and
+        with resident stepping;
       - fp32 atomic accumulation (the benchmark's mode): rasters bit-exact for
         the first 100 steps, state within 1e-5 relative at the last snapshot
         before the first differing step, population rate and ISI-CV within
@@ -65,10 +66,14 @@ def _oracle_net(csr, dtype=np.float32):
     return oracle.OracleNet(n, p, D, pops, csr, state=init_state(n, p, SEED), dtype=dtype)
 
 
-@pytest.mark.parametrize("tiles", [0, 1, 2], ids=["block_tiles", "warp_tiles", "persistent_block_tiles"])
+@pytest.mark.parametrize("tiles", [0, 1, 2, "resident"],
+                         ids=["block_tiles", "warp_tiles", "persistent_block_tiles", "resident"])
 def test_full_size_fixed_point_equals_oracle(ctx, full_csr, tiles):
     net = _bench_net(ctx, True)
-    net.set_update_tiles(tiles, 2 if tiles == 1 else 0)
+    if tiles == "resident":
+        net.set_resident(True)
+    else:
+        net.set_update_tiles(tiles, 2 if tiles == 1 else 0)
     r_gpu = net.run(100)
     on = _oracle_net(full_csr)
     r_orc, ev = on.run(100, acc_mode=oracle.ACC_FIXED, nthreads=THREADS)
