@@ -356,6 +356,12 @@ int szsnn_net_timing(szsnn_net* net, double* propagate_ms, double* update_ms, do
  * warp (8/16/32); propagate grid blocks (0 = 16 per SM); update block size
  * (threads, a multiple of 32 in 32..256; each thread updates 4 units) */
 int szsnn_net_set_tuning(szsnn_net* net, int propagate_mode, int group, int propagate_blocks, int update_block);
+/* Units each update thread handles per step (1..16; 0 = automatic: 4 while
+ * the network gives at least four update blocks per SM, fewer below).  A
+ * block's tile is update_block x units; fewer, longer blocks trade the
+ * launch's trailing partial wave for longer blocks.  Results are identical
+ * for every value. */
+int szsnn_net_set_update_units(szsnn_net* net, int units_per_thread);
 /* Update tiles: mode 0 = one tile per update block, a new block per tile each
  * step; mode 1 = persistent warp tiles: blocks_per_sm update blocks per SM
  * (0 = 2), each warp streaming 128-unit tiles through a two-stage ring of

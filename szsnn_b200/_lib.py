@@ -140,6 +140,7 @@ SIGNATURES = {
     "szsnn_net_set_tuning": (_I, [_P, _I, _I, _I, _I]),
     "szsnn_net_set_update_tiles": (_I, [_P, _I, _I]),
     "szsnn_net_set_resident": (_I, [_P, _I, _I, _I]),
+    "szsnn_net_set_update_units": (_I, [_P, _I]),
     "szsnn_net_set_overlap": (_I, [_P, C.c_int]),
     "szsnn_step_static": (_I, [_P, C.c_char_p, C.c_size_t]),
     "szsnn_probe_peaks": (_I, [_P, _I64, _P]),

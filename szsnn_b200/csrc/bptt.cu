@@ -211,7 +211,7 @@ struct BpttBwd {
     float* lam_e;      // [B][N] total dL/dIe of step t+1, then of step t
     float* lam_i;
     float* lamS;       // [2N][Bp] this step's (lam_e; lam_i), trial-minor
-    float* lamT;       // [2][B][N] the same, neuron-minor
+    float* lamT;       // [2][B][N] the same, neuron-minor (this step's parity half of a [2][2][B][N] buffer)
     const float* R;    // [N][Bp] recurrent term from step t+1
     float* lam_y;      // [B][K] of this step
     const float* lam_y_next;  // [B][K] of step t+1
@@ -407,7 +407,7 @@ Work layout(const szsnn_bptt_desc* d)
     w.Ie = take(BN); w.Ii = take(BN); w.v = take(BN); w.y = take(BK);
     w.u_seg = take((size_t)d->checkpoint_every * BN);
     w.lam_u = take(BN); w.lam_e = take(BN); w.lam_i = take(BN);
-    w.lamS0 = take(2 * NBp); w.lamS1 = take(2 * NBp); w.lamT = take(2 * BN);
+    w.lamS0 = take(2 * NBp); w.lamS1 = take(2 * NBp); w.lamT = take(4 * BN);
     w.R = take(NBp); w.ly0 = take(BK); w.ly1 = take(BK);
     w.colsel = take((size_t)d->nnz);  // ints, same size as floats
     w.total = o * sizeof(float);
@@ -551,7 +551,7 @@ extern "C" int szsnn_bptt_backward(const szsnn_bptt_desc* d, char* err, size_t e
     float* lamY[2] = {ws + w.ly0, ws + w.ly1};
     int* col_sel = reinterpret_cast<int*>(ws + w.colsel);
     g.lam_u = ws + w.lam_u; g.lam_e = ws + w.lam_e; g.lam_i = ws + w.lam_i;
-    g.lamT = ws + w.lamT; g.R = ws + w.R; g.col_sel = col_sel; g.Bp = Bp;
+    g.R = ws + w.R; g.col_sel = col_sel; g.Bp = Bp;
     g.g_ymax = d->g_ymax; g.g_vsum = d->g_vsum;
     g.dw_in = d->dw_in; g.dw_rec = d->dw_rec; g.dw_out = d->dw_out;
     for (float* p : {g.lam_u, g.lam_e, g.lam_i})
@@ -581,6 +581,28 @@ extern "C" int szsnn_bptt_backward(const szsnn_bptt_desc* d, char* err, size_t e
     if (stored) k.u_seg = d->u_trace;
     const int seg_len = stored ? d->T : d->checkpoint_every;
     const int nseg = (d->T + seg_len - 1) / seg_len;
+    // dWin(t) reads only lambda_t (lamT of t's parity), so it runs on a side
+    // stream beside spmm(t-1); adjoint(t-2), which rewrites that parity half,
+    // waits for it.  dW_in keeps its order of accumulation (t descending, one
+    // stream).  With per-phase timing the phases stay on one stream.
+    const bool side = d->phase_ms == nullptr;
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_lam[2] = {}, ev_dw[2] = {};
+    struct Release {
+        cudaStream_t* s; cudaEvent_t* a; cudaEvent_t* b;
+        ~Release() { for (int p = 0; p < 2; ++p) { if (a[p]) cudaEventDestroy(a[p]); if (b[p]) cudaEventDestroy(b[p]); }
+                     if (*s) cudaStreamDestroy(*s); }
+    } release{&st2, ev_lam, ev_dw};
+    if (side) {
+        BP_TRY(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        for (int p = 0; p < 2; ++p) {
+            BP_TRY(cudaEventCreateWithFlags(&ev_lam[p], cudaEventDisableTiming));
+            BP_TRY(cudaEventCreateWithFlags(&ev_dw[p], cudaEventDisableTiming));
+        }
+        BP_TRY(cudaEventRecord(ev_dw[0], st));  // the side stream starts after the set-up above
+        BP_TRY(cudaStreamWaitEvent(st2, ev_dw[0], 0));
+    }
+    bool dw_pending[2] = {false, false};
     for (int seg = nseg - 1; seg >= 0; --seg) {
         const int t0 = seg * seg_len, t1 = std::min(d->T, t0 + seg_len);
         if (!stored) {
@@ -608,13 +630,28 @@ extern "C" int szsnn_bptt_backward(const szsnn_bptt_desc* d, char* err, size_t e
             g.lamS = lamS[par];
             g.lam_y = lamY[par];
             g.lam_y_next = lamY[par ^ 1];
+            g.lamT = ws + w.lamT + (size_t)par * 2 * BN;
+            if (dw_pending[par]) BP_TRY(cudaStreamWaitEvent(st, ev_dw[par], 0));  // dWin(t+2) done with this half
             k_bptt_adjoint<<<grid, BP_BLOCK, 0, st>>>(k, g, t, t0, have_R ? 1 : 0);
             BP_TRY(cudaGetLastError());
             pt.mark(2);
-            k_bptt_dwin<<<grid_in, BP_BLOCK, 0, st>>>(k, g, t);
-            BP_TRY(cudaGetLastError());
+            if (side) {
+                BP_TRY(cudaEventRecord(ev_lam[par], st));
+                BP_TRY(cudaStreamWaitEvent(st2, ev_lam[par], 0));
+                k_bptt_dwin<<<grid_in, BP_BLOCK, 0, st2>>>(k, g, t);
+                BP_TRY(cudaGetLastError());
+                BP_TRY(cudaEventRecord(ev_dw[par], st2));
+                dw_pending[par] = true;
+            } else {
+                k_bptt_dwin<<<grid_in, BP_BLOCK, 0, st>>>(k, g, t);
+                BP_TRY(cudaGetLastError());
+            }
             pt.mark(3);
         }
+    }
+    if (side) {  // the caller's stream resumes after the last dWin
+        BP_TRY(cudaEventRecord(ev_dw[0], st2));
+        BP_TRY(cudaStreamWaitEvent(st, ev_dw[0], 0));
     }
     BP_TRY(pt.finish());
     return SZSNN_OK;

@@ -41,7 +41,8 @@
 // (IF models), computed once on the host with the same fp32 operations
 #define POP_SLOTS 16
 #define INLINE_POPS 4
-#define UPD_UPT 4        // most units per update thread (strided by the block size)
+#define UPD_UPT 4        // units per update thread chosen by default (strided by the block size)
+#define UPD_MAX_UPT 16   // most units per update thread szsnn_net_set_update_units accepts
 #define UPD_MAX_BLOCK 256  // update threads per block (the step kernel's block too)
 #define UPD_MIN_BLOCKS 6   // resident blocks of UPD_MAX_BLOCK per SM the register budget keeps
 struct PopDev {
@@ -86,7 +87,7 @@ struct NetDev {
     unsigned long long* group_spikes;      // [n_groups]
     const int2* blk_pop;                   // per update block: (first overlapping pop, count)
     uint32_t par0;                         // parity of the step counter when the launch runs
-    int32_t upt;                           // units per update thread (1..UPD_UPT)
+    int32_t upt;                           // units per update thread (1..UPD_MAX_UPT)
     int32_t ib_lo[INLINE_POPS], ib_hi[INLINE_POPS];  // update blocks [lo, hi) lying inside slot i (empty: none)
     PopDev ipop[INLINE_POPS];              // populations with shared parameters, by value in the kernel parameters
     uint32_t tiles;                        // update tile scheme: 0 a block per tile, 1 persistent warp tiles,
@@ -151,6 +152,7 @@ struct szsnn_net {
     uint64_t graph_launches = 0, kernel_launches = 0;
     int prop_mode = 0, prop_group = 16, prop_blocks = 0, upd_block = 256;
     int upd_tiles = 0, upd_per_sm = 0;   // update tiles: 0 block tiles, 1 persistent warp tiles (blocks per SM)
+    int upd_units = 0;                   // units per update thread (0: automatic, upd_upt)
     int64_t own_lo[2] = {0, 0}, own_hi[2] = {-1, -1};  // owned neuron / source ranges (-1: all)
     double t_prop_ms = 0, t_upd_ms = 0, t_total_ms = 0;
     cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;  // around the last szsnn_net_run*
@@ -1752,6 +1754,7 @@ int num_sms(szsnn_ctx* ctx) { return ctx->num_sms > 0 ? ctx->num_sms : 148; }
 // and more blocks in parallel shorten it.
 int upd_upt(const szsnn_net* n)
 {
+    if (n->upd_units > 0) return n->upd_units;
     const int64_t per_sm = sz_div_up(n->U, (int64_t)num_sms(n->ctx) * n->upd_block);  // blocks per SM at 1 unit
     return (int)std::max<int64_t>(1, std::min<int64_t>(UPD_UPT, per_sm / 4));
 }
@@ -2837,6 +2840,25 @@ extern "C" int szsnn_net_set_tuning(szsnn_net* n, int mode, int group, int block
     return SZSNN_OK;
 }
 
+extern "C" int szsnn_net_set_update_units(szsnn_net* n, int units_per_thread)
+{
+    if (!n) return SZSNN_ERR_ARG;
+    if (units_per_thread < 0 || units_per_thread > UPD_MAX_UPT)
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "units per update thread must be in 0..16 (0: automatic)");
+    const int old = n->upd_units;
+    n->upd_units = units_per_thread;
+    // a block tile must fit the shared memory of one block
+    const size_t bytes = tile_smem_bytes((int64_t)upd_upt(n) * n->upd_block, n->acc_mode == SZSNN_ACC_FIXED);
+    if (bytes > 200 * 1024) {
+        n->upd_units = old;
+        return szsnn_set_error(n->ctx, SZSNN_ERR_ARG, "the update block's tile exceeds shared memory");
+    }
+    NET_TRY(n, fill_blk_pop(n));
+    for (auto& kv : n->graphs) cudaGraphExecDestroy(kv.second);
+    n->graphs.clear();
+    return SZSNN_OK;
+}
+
 extern "C" int szsnn_net_set_update_tiles(szsnn_net* n, int mode, int blocks_per_sm)
 {
     if (!n) return SZSNN_ERR_ARG;
@@ -3236,6 +3258,8 @@ extern "C" int szsnn_step_static(const szsnn_static_step* s, char* err, size_t e
     d.stats = (unsigned long long*)(base + 64);
     d.err = s->error_word;
     d.upt = 1;
+    d.own_lo[0] = 0; d.own_hi[0] = N;  // every unit is updated here
+    d.own_lo[1] = N; d.own_hi[1] = U;
     k_propagate<16><<<sms * 16, 256, 0, st>>>(d, 0, 1, PF_ZERO_SLOT | PF_SPIKES);
     e = cudaGetLastError();
     if (e == cudaSuccess) {

@@ -243,6 +243,10 @@ class Network:
         persistent block tiles (`blocks_per_sm`, 0: as many as stay resident)."""
         L.check(self.lib.szsnn_net_set_update_tiles(self.h, mode, blocks_per_sm), self.ctx.h, "set_update_tiles")
 
+    def set_update_units(self, units_per_thread: int) -> None:
+        """Units per update thread (0: automatic)."""
+        L.check(self.lib.szsnn_net_set_update_units(self.h, units_per_thread), self.ctx.h, "set_update_units")
+
     def set_resident(self, on: bool, update_warps: int = 0, blocks: int = 0) -> None:
         """Resident stepping: each run chunk is one cooperative launch that
         keeps the neurons' state in shared memory across its steps

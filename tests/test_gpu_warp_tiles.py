@@ -13,7 +13,8 @@ population boundary run the generic per-unit update.  Covered:
     short and its bulk transfers are rounded to 16 bytes);
   * populations whose boundaries fall inside warp tiles (generic tiles);
   * switching between the three schemes mid-run;
-  * fp32 accumulation with dyadic weights (exact sums in any order).
+  * fp32 accumulation with dyadic weights (exact sums in any order);
+  * block tiles of 1, 2, 5 and 8 units per thread (szsnn_net_set_update_units).
 Persistent block tiles take the block tiles of mode 0 in turn, one mbarrier
 phase per loaded tile, in blocks that stay resident for the whole launch.
 """
@@ -161,4 +162,28 @@ def test_warp_tiles_switch_mid_run_and_float_dyadic(ctx):
     for k in range(4):
         assert np.array_equal(net.get_state(k), on.state[k])
     assert net.stats()["events"] == ev
+    net.close()
+
+
+@pytest.mark.parametrize("units", [1, 2, 5, 8])
+def test_update_units_per_thread_equal_oracle(ctx, units):
+    """szsnn_net_set_update_units: longer or shorter block tiles (block size
+    x units), including tiles that do not divide the populations, give the
+    oracle's rasters and state bit for bit."""
+    n, p, D = 60_000, 6_000, 16
+    blocks, pops, st = cond_network(n, p, fanout=40, D=D, seed=10)
+    net = sz.Network(ctx, n, p, D, pops, state=st, acc_mode=L.ACC_FIXED, graph_chunk=25)
+    net.generate(blocks, seed=79)
+    net.set_tuning(1, 16, 296, 128)
+    net.set_update_units(units)
+    on = oracle.OracleNet(n, p, D, pops, oracle.generate(blocks, 79, n + p, D), state=st)
+    r = net.run(60)
+    ro, ev = on.run(60, acc_mode=oracle.ACC_FIXED)
+    assert _spikes(ro) > 1000
+    assert np.array_equal(r, ro)
+    for k in range(4):
+        assert np.array_equal(net.get_state(k), on.state[k])
+    assert net.stats()["events"] == ev
+    with pytest.raises(sz.SzsnnError):
+        net.set_update_units(17)
     net.close()
