@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(BP_BLOCK) k_bptt_spmm(BpttK k, const int* __re
         const float w = kk < e ? __ldg(&k.val[kk]) : 0.0f;
         const int cs = kk < e ? __ldg(&col_sel[kk]) : 0;
         const float dw_old = (mask && kk < e && w != 0.0f) ? dw[kk] : 0.0f;
-#pragma unroll 4
+#pragma unroll  // all 16 synapse pairs of the chunk: their lambda loads in flight together
         for (int q = 0; q < 32; q += 2) {
             const float wq = __shfl_sync(0xffffffffu, w, q + half);
             const int cq = __shfl_sync(0xffffffffu, cs, q + half);
