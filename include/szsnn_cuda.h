@@ -379,8 +379,8 @@ int szsnn_net_set_update_tiles(szsnn_net* net, int mode, int blocks_per_sm);
  * other warps take their share of the far delivery.  Same step order,
  * arithmetic and results as the overlapped graphs (bit-identical in
  * fixed-point accumulation).  Needs the overlapped order, at most four
- * populations with shared parameters (IF_curr_exp, IF_cond_exp, Izhikevich
- * neurons; Poisson sources), no state monitor, and a block's neuron state
+ * populations (IF_curr_exp, IF_cond_exp, Izhikevich neurons; Poisson
+ * sources; shared or per-unit parameters), no state monitor, and a block's neuron state
  * within shared memory (about 1.6M IF neurons on one B200); otherwise
  * SZSNN_ERR_ARG with the reason, and a later run whose network no longer
  * qualifies fails with SZSNN_ERR_STATE.  szsnn_net_step and the profiling

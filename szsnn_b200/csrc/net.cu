@@ -1478,6 +1478,7 @@ __device__ __forceinline__ void res_update(const NetDev& nd, const PopDev* __res
             }
         const int p0 = __reduce_max_sync(0xffffffffu, mine);
         uni = __all_sync(0xffffffffu, uni && (mine == -2 || mine == p0)) && p0 >= 0;
+        if (uni && sp[p0].pn) uni = false;  // per-unit parameter tables: unit by unit
         if (uni) {
             const PopDev& P = sp[p0];
             if (P.model == SZSNN_IF_COND_EXP)
@@ -1500,15 +1501,20 @@ __device__ __forceinline__ void res_update(const NetDev& nd, const PopDev* __res
                 if (id[u] < N) {
                     float v = st[0][(id[u] - n_lo)], g1 = st[1][(id[u] - n_lo)], g2 = 0.0f, fr = 0.0f;
                     if (P.model != SZSNN_IZHIKEVICH) { g2 = st[2][(id[u] - n_lo)]; fr = st[3][(id[u] - n_lo)]; }
-                    spk[u] = run_neuron(SharedParams{P.p}, P.model, P.flags, v, g1, g2, fr, in_e[u], in_i[u], ext[u],
-                                        f[u]);
+                    if (P.pn)
+                        spk[u] = run_neuron(UnitParams{P.pn, (int64_t)id[u] - P.begin, P.end - P.begin}, P.model,
+                                            P.flags, v, g1, g2, fr, in_e[u], in_i[u], ext[u], f[u]);
+                    else
+                        spk[u] = run_neuron(SharedParams{P.p}, P.model, P.flags, v, g1, g2, fr, in_e[u], in_i[u],
+                                            ext[u], f[u]);
                     st[0][(id[u] - n_lo)] = v;
                     st[1][(id[u] - n_lo)] = g1;
                     if (P.model != SZSNN_IZHIKEVICH) { st[2][(id[u] - n_lo)] = g2; st[3][(id[u] - n_lo)] = fr; }
                     if (FIXED) { inb.fe[id[u]] = 0; inb.fi[id[u]] = 0; }
                     else { inb.e[id[u]] = 0.0f; inb.i[id[u]] = 0.0f; }
                 } else if (P.model == SZSNN_POISSON) {
-                    spk[u] = sz_poisson_fires(P.seed, (int64_t)id[u] - P.begin, t, P.p[0]) || f[u];
+                    const float prob = P.pn ? P.pn[(int64_t)id[u] - P.begin] : P.p[0];
+                    spk[u] = sz_poisson_fires(P.seed, (int64_t)id[u] - P.begin, t, prob) || f[u];
                 }
             }
         }
@@ -2020,7 +2026,6 @@ bool res_check(szsnn_net* n, std::string* why, size_t* smem, int* nst)
     for (const PopDev& q : n->h_pops) {
         const bool neuron_model = q.model == SZSNN_IF_CURR_EXP || q.model == SZSNN_IF_COND_EXP ||
                                   q.model == SZSNN_IZHIKEVICH;
-        if (q.pn) return no("resident stepping needs shared population parameters");
         if (q.begin < n->N && q.end > n->N) return no("a population spans neurons and sources");
         if (q.begin < n->N && !neuron_model) return no("neurons of a source model");
         if (q.begin >= n->N && q.model != SZSNN_POISSON) return no("sources other than Poisson");

@@ -15,6 +15,7 @@ warps share every block, and a bounded grid barrier ends each step.  Covered:
   * switching between resident chunks and the per-step graphs mid-run, and
     single steps (szsnn_net_step) between resident runs;
   * fp32 accumulation with dyadic weights (exact sums in any order);
+  * per-unit parameter tables (the 1000-neuron Izhikevich network);
   * the networks resident stepping refuses, with the reason.
 """
 import numpy as np
@@ -166,16 +167,42 @@ def test_resident_switch_mid_run_single_steps_float_dyadic(ctx):
     net.close()
 
 
+def test_resident_per_unit_izhikevich_equals_oracle(ctx):
+    """The 1000-neuron Izhikevich network with per-neuron a, b, c, d (per-unit
+    parameter tables, updated unit by unit), thalamic current, half-steps."""
+    from szsnn_b200 import workloads as WL
+    izh = WL.izh_network(n=1000, seed=5)
+    pops, csr, st = WL.izh_native(izh)
+    pops[0].flags = sz.POP_IZH_HALF_STEPS
+    steps = 300
+    cur = WL.thalamic(1000, izh["ne"], steps, seed=9)
+    net = sz.Network(ctx, 1000, 0, izh["D"], pops, csr=csr, state=st, acc_mode=L.ACC_FIXED, graph_chunk=100)
+    net.set_resident(True)
+    dcur = ctx.upload(cur)
+    raster = ctx.buffer(steps * net.words * 4)
+    net.run_device(steps, current_ptr=dcur.ptr, raster_ptr=raster.ptr)
+    r = raster.read(np.uint32, steps * net.words).reshape(steps, net.words)
+    on = oracle.OracleNet(1000, 0, izh["D"], pops, csr, state=st)
+    ro, ev = on.run(steps, current=cur, acc_mode=oracle.ACC_FIXED)
+    _check(net, on, r, ro, ev, slots=2)
+    dcur.free()
+    raster.free()
+    net.close()
+
+
 def test_resident_refusals(ctx):
     n = 2000
     net_ = if_network(n=n, n_syn=20 * n, max_delay=8, dyadic=True, seed=2)
     csr = sz.csr_from_synapses(n, 8, net_["src"], net_["tgt"], net_["w"], net_["d1"])
     st = [net_["v0"], None, None, np.full(n, 1e4, np.float32)]
-    pn = np.tile(np.array(net_["pv"], np.float32)[:, None], (1, n))
-    per_unit = sz.Network(ctx, n, 0, 8, [sz.Pop(sz.IF_CURR_EXP, 0, n, net_["pv"], per_unit=pn)], csr=csr, state=st)
-    with pytest.raises(sz.SzsnnError, match="shared population parameters"):
-        per_unit.set_resident(True)
-    per_unit.close()
+    const = sz.Network(ctx, n, 32, 8, [sz.Pop(sz.IF_CURR_EXP, 0, n, net_["pv"]),
+                                       sz.Pop(sz.CONST_RATE, n, n + 32, np.array([7.0], np.float32))],
+                       csr=sz.csr_from_synapses(n + 32, 8, net_["src"], net_["tgt"], net_["w"], net_["d1"]),
+                       state=[np.concatenate([net_["v0"], np.zeros(32, np.float32)]), None, None,
+                              np.concatenate([np.full(n, 1e4, np.float32), np.zeros(32, np.float32)])])
+    with pytest.raises(sz.SzsnnError, match="sources other than Poisson"):
+        const.set_resident(True)
+    const.close()
     net = sz.Network(ctx, n, 0, 8, [sz.Pop(sz.IF_CURR_EXP, 0, n, net_["pv"])], csr=csr, state=st)
     net.set_overlap(False)
     with pytest.raises(sz.SzsnnError, match="overlapped"):
