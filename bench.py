@@ -288,11 +288,19 @@ def bench_configs(ctx, args):
                 "bound": "launch and latency: one fused kernel per step over a few thousand units"}
 
     def best_run(net, steps, n_units, bytes_per_unit, current_ptr=None):
-        """The per-step graphs, then resident stepping (one cooperative launch
-        per 100 steps) at a few grid sizes; the fastest is reported as `gpu`,
-        every timing beside it."""
-        runs = {"graphs": gpu_run(net, steps, n_units, bytes_per_unit, current_ptr)}
+        """The per-step graphs at the default and at the tuned launch shape,
+        then resident stepping (one cooperative launch per 100 steps) at a few
+        grid sizes; the fastest is reported as `gpu`, every timing beside it."""
+        runs = {"graphs_default_shape": gpu_run(net, steps, n_units, bytes_per_unit, current_ptr)}
+        from szsnn_b200.autotune import tune
+        ch = tune(net, replays=50, use_cache=False)  # order and launch shape on replays of the warmed-up step
+        live = refine_live(net, ctx, ch, 4, current_ptr=current_ptr) if ch["overlap"] else None
+        runs["graphs_tuned"] = gpu_run(net, steps, n_units, bytes_per_unit, current_ptr)
+        runs["graphs_tuned"]["shape"] = live["chosen"] if live else {
+            k: ch[k] for k in ("overlap", "mode", "group", "blocks", "update_block")}
         for blocks in (0, 32, 8):
+            if not net.overlap:  # the tuner chose the classic order, which resident stepping does not run
+                break
             try:
                 net.set_resident(True, 16, blocks)
             except Exception as e:
@@ -522,7 +530,7 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def refine_live(net, ctx, ch, k, steps=1000, warm=200):
+def refine_live(net, ctx, ch, k, steps=1000, warm=200, current_ptr=None):
     """The tuner ranks shapes on replays of one step; the live step (a
     different spike pattern each step, the graphs' back-to-back launches)
     can order them differently.  The k best overlapped shapes by replay time
@@ -541,9 +549,9 @@ def refine_live(net, ctx, ch, k, steps=1000, warm=200):
     live = []
     for mode, group, blocks, ub in cand:
         net.set_tuning(mode, group, blocks, ub)
-        net.run_device(warm)
+        net.run_device(warm, current_ptr=current_ptr)
         ctx.sync()
-        net.run_device(steps)
+        net.run_device(steps, current_ptr=current_ptr)
         ctx.sync()
         live.append((net.device_ms() / steps * 1e3, (mode, group, blocks, ub)))
     best = min(live)
