@@ -49,15 +49,11 @@ CPU_WARM_STEPS = 500     # oracle warm-up simulation steps (past the v(0) volley
 CPU_TIMED_STEPS = 200    # simulation steps timed by the cpu_baseline leg
 BYTES_PER_EVENT = 8      # int32 target + fp32 weight, delay implied by the bucket
 BYTES_PER_NEURON = 48    # 16 B state read + 16 B write + 8 B input read + 8 B clear
-# DRAM bytes (read + write) per launch from single ncu captures (cold L2):
-# k_update at 1.1M units, the benchmark's unit count; k_propagate at 300k
-# neurons x 1000 synapses (152,640 events per launch), scaled by events.
-NCU_UPDATE_TRAFFIC = 25_399_040
-NCU_PROPAGATE_TRAFFIC_PER_EVENT = 5_706_752 / 152_640
-# k_step at 1.1M units and fan-out 100 (245,471 events per launch): 70.7 MB; the per-(spike, delay)
-# item traffic is the same at fan-out 1000, each further event adds its 8 B synapse
-NCU_STEP_TRAFFIC_FANOUT100 = 70_680_320
-NCU_STEP_EVENTS_FANOUT100 = 245_471
+# k_step of the benchmark network itself (1M x 1000, fp32, the tuned shape), L2 left warm as in the
+# timed run (ncu --cache-control none, one-pass DRAM counters, mean of three launches in the timed
+# region): 3.88 MB per launch, about the ~500k synapses the step delivers; the neuron state, ring and
+# bucket index stay in L2
+NCU_STEP_TRAFFIC_WARM = 3_882_752
 
 
 def parse(argv=None):
@@ -733,8 +729,8 @@ def main():
     # every unit, the delay-1 buckets of its spikes and the delay >= 2
     # delivery of the next step) in the overlapped order; its live time per
     # launch is the timed region's time per simulation step
-    traffic = (int(NCU_STEP_TRAFFIC_FANOUT100 + max(0.0, ev_step - NCU_STEP_EVENTS_FANOUT100) * 8)
-               if (n + p == 1_100_000 and overlap and not res_on) else None)
+    traffic = (NCU_STEP_TRAFFIC_WARM
+               if (n + p == 1_100_000 and args.fanout == 1000 and overlap and not res_on) else None)
     achieved = step_bytes / (us_live * 1e-6) / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "traffic": traffic,
@@ -748,6 +744,8 @@ def main():
                 "atomic_frac": round(ev_step / (us_live * 1e-6) / chip["red_per_s"], 4),
                 "ceilings": "l2_gbs_peak: L2-resident copy of 2 x 16 MB; atomic_per_s_peak: random fp32 red into "
                             "2 x N floats (szsnn_probe_peaks, this device, this run)",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_step on this workload, L2 "
+                                  "warm as in the timed run (--cache-control none), mean of three launches",
                 "replays": {"step_us": round(step_us, 3), "order": "overlapped" if overlap else "classic",
                             "of": "the per-step launches (k_step) on scratch state" if res_on else "the timed kernels",
                             "delivery_alone_us": round(prop_us, 3), "delivery_events": ev_launch,
