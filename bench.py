@@ -85,7 +85,8 @@ def parse(argv=None):
                          "memory): auto keeps it when its live step time beats the tuned graphs'")
     ap.add_argument("--resident-warps", default="12,16,20,24",
                     help="update warps per block the resident choice tries")
-    ap.add_argument("--e2e-steps", type=int, default=2000)
+    ap.add_argument("--e2e-steps", type=int, default=5000,
+                    help="simulation steps of the end-to-end run (host input words in, raster out, every step)")
     ap.add_argument("--profile-steps", type=int, default=200)
     ap.add_argument("--cpu-neurons", type=int, default=None,
                     help="neurons of the network the CPU port runs (default: the benchmark's own --neurons)")
