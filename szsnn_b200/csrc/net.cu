@@ -588,7 +588,9 @@ struct UnitIn {
 // memory rather than by registers.  Each thread then updates units
 // j * blockDim.x + threadIdx.x of the tile from shared memory, with the
 // population's parameters as constant-bank operands (slot and model
-// compile-time), and stores state and cleared inputs straight to global.
+// compile-time), writing the new state and the cleared inputs back into
+// the tile; after the last sub-tile one bulk store per array returns the
+// tile to global memory.
 // Dynamic shared memory: mbarrier at 0, arrays from byte 16: st0..st3 (T
 // floats each), then the exc / inh inputs (T floats or T int64 each).
 __host__ __device__ __forceinline__ size_t tile_smem_bytes(int64_t T, bool fixed)
@@ -623,6 +625,17 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  :: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
 }
+
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                 :: "l"(dst), "r"(smem_addr(src)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// the issuing thread's bulk stores have read their shared-memory sources
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
 {
@@ -695,13 +708,13 @@ __device__ __forceinline__ bool tile_unit(const NetDev& nd, const PopDev& P, con
     if (FIXED) {
         in_e = __ll2float_rn(sm.fe[u]) * (1.0f / 4294967296.0f);
         in_i = __ll2float_rn(sm.fi[u]) * (1.0f / 4294967296.0f);
-        inb.fe[id] = 0;
-        inb.fi[id] = 0;
+        sm.fe[u] = 0;
+        sm.fi[u] = 0;
     } else {
         in_e = sm.ie[u];
         in_i = sm.ii[u];
-        inb.e[id] = 0.0f;
-        inb.i[id] = 0.0f;
+        sm.ie[u] = 0.0f;
+        sm.ii[u] = 0.0f;
     }
     const float i_ext = current ? current[id] : 0.0f;
     if (nd.dbg_in_e) { nd.dbg_in_e[id] = in_e; nd.dbg_in_i[id] = in_i; }
@@ -710,9 +723,9 @@ __device__ __forceinline__ bool tile_unit(const NetDev& nd, const PopDev& P, con
     if (MODEL == SZSNN_IF_CURR_EXP) spk = sz_if_curr_exp(sp, v, g1, g2, fr, in_e, in_i, i_ext, f, sp(12), sp(13));
     else if (MODEL == SZSNN_IF_COND_EXP) spk = sz_if_cond_exp(sp, v, g1, g2, fr, in_e, in_i, i_ext, f, sp(12), sp(13));
     else spk = sz_izhikevich(sp, v, g1, in_e, in_i, i_ext, f, (P.flags & SZSNN_POP_IZH_HALF_STEPS) != 0);
-    nd.st0[id] = v;
-    nd.st1[id] = g1;
-    if (MODEL != SZSNN_IZHIKEVICH) { nd.st2[id] = g2; nd.st3[id] = fr; }
+    sm.st[0][u] = v;
+    sm.st[1][u] = g1;
+    if (MODEL != SZSNN_IZHIKEVICH) { sm.st[2][u] = g2; sm.st[3][u] = fr; }
     return spk;
 }
 
@@ -735,6 +748,29 @@ __device__ __forceinline__ void tile_run(const NetDev& nd, const InBuf& inb, int
         if (ok && id < nd.U && owned(nd, id)) spk = tile_unit<MODEL, FIXED>(nd, P, inb, sm, (uint32_t)id, u, t, forced, current);
         __syncwarp();
         update_spikes(nd, t, id, spk, lane, out_words);
+    }
+    // the tile's new state and cleared inputs, back to global memory from
+    // shared memory in one bulk store per array (units not updated here are
+    // stored back as they were loaded)
+    if (MODEL == SZSNN_POISSON) return;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the threads' writes, to the bulk copy engine
+    if (!__syncthreads_and(ok ? 1 : 0)) return;  // a tile whose copies timed out is not stored (block-uniform)
+    if (threadIdx.x == 0) {
+        const int64_t n = min((int64_t)T, nd.U - tile0);
+        const uint32_t b4 = (uint32_t)((n * 4 + 15) & ~(int64_t)15);
+        const uint32_t b8 = (uint32_t)((n * 8 + 15) & ~(int64_t)15);
+        const int nst = MODEL == SZSNN_IZHIKEVICH ? 2 : 4;
+        float* const gst[4] = {nd.st0, nd.st1, nd.st2, nd.st3};
+        for (int k = 0; k < nst; ++k) bulk_store(gst[k] + tile0, sm.st[k], b4);
+        if (FIXED) {
+            bulk_store(inb.fe + tile0, sm.fe, b8);
+            bulk_store(inb.fi + tile0, sm.fi, b8);
+        } else {
+            bulk_store(inb.e + tile0, sm.ie, b4);
+            bulk_store(inb.i + tile0, sm.ii, b4);
+        }
+        bulk_commit();
+        bulk_wait_read();  // the sources are read before the block leaves or reloads its tile
     }
 }
 
@@ -950,17 +986,6 @@ __device__ __forceinline__ int wt_slot(const NetDev& nd, int64_t u0)
         if (nd.ipop[i].end > nd.ipop[i].begin && u0 >= nd.ipop[i].begin && u1 <= nd.ipop[i].end) return i;
     return -1;
 }
-
-__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes)
-{
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
-                 :: "l"(dst), "r"(smem_addr(src)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-
-// the issuing thread's bulk stores have read their shared-memory sources
-__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
 {
